@@ -1,0 +1,409 @@
+#!/usr/bin/env python
+"""Benchmark of the TagMatch subset-matching hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (config1 shapes): 10,000,000 stored 192-bit filters from the seeded
+generator (seed 2, tag sets of 1-8 Zipf(1.0) tags over 100,000 tags, 7 bits
+per tag, 1-4 keys per filter), partitions of at most 65,536 filters, and
+1,000,000 queries per GPU per step, matched in per-partition batches of 256
+queries.  A step is one pass of `match` over the step's queries.
+
+* value: queries/s with the queries already resident in HBM (device API),
+  timed with CUDA events on the matcher's stream, max over ranks.
+* e2e: the same through the host C ABI (tm_match_batch): host->device copy
+  of the queries and device->host copy of every result key inside the timed
+  region.
+* roofline: the subset-test kernel's algorithmic bytes per launch over its
+  CUDA-event duration, against the measured HBM copy bandwidth.
+* cpu_baseline: the oracle's C port of the reference matcher on this host's
+  cores, on a bounded sample of the same queries.
+
+--impl reference times the reference's own sequential matcher (test_matcher,
+built from the reference sources into oracle/_ref), one process per host
+core over shards of a query sample, on the same table.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "queries/s at 10M 192-bit filters (bit-exact) and p50/p99 latency vs plain GPU"
+UNIT = "queries/s"
+FILTERS = 10_000_000
+QUERIES = 1_000_000
+SEED = 2
+MAX_P = 65_536
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--filters", type=int, default=FILTERS)
+    ap.add_argument("--queries", type=int, default=QUERIES)
+    ap.add_argument("--batch", type=int, default=131072, help="queries per device batch")
+    ap.add_argument("--unique", action="store_true", help="time match_unique instead of match")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            rows = open(self.path).read().strip().splitlines()
+        except OSError:
+            rows = []
+        for r in rows:
+            t = [x.strip() for x in r.split(",")]
+            if len(t) < 9:
+                continue
+            try:
+                sm.append(float(t[1]))
+                mx.append(float(t[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, t[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if self.path:
+            os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        kw = {}
+        if backend == "nccl":
+            import torch
+            kw["device_id"] = torch.device("cuda", local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=900), **kw)
+    return world, rank, local
+
+
+def max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def shard_seed(rank):
+    """Rank 0 matches the configuration's own query stream; others get their own."""
+    return SEED if rank == 0 else SEED + 7919 * rank
+
+
+def cpu_baseline(f, ko, k, q, seconds):
+    """The oracle's C port of test_matcher on all host cores, bounded sample."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    n = max(cores, 8)
+    t0 = time.perf_counter()
+    oracle.match(f, ko, k, q[:n], threads=cores)
+    dt = time.perf_counter() - t0
+    per_q = dt / n
+    m = int(min(q.shape[0], max(n, seconds / max(per_q, 1e-9))))
+    t0 = time.perf_counter()
+    oracle.match(f, ko, k, q[:m], threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {m} of the step's queries against the full {f.shape[0]}-filter table "
+                      f"(oracle/oracle.c restatement of test_matcher.cc:74-81), {dt:.1f} s"}
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    from tagmatch_b200 import TagMatch, workload
+
+    t0 = time.perf_counter()
+    f, ko, k = workload.generate_filters(args.filters, SEED)
+    q = workload.generate_queries(args.queries, f, shard_seed(rank))
+    t_gen = time.perf_counter() - t0
+    tm = TagMatch()
+    tm.set_persistence(False)
+    t0 = time.perf_counter()
+    tm.add_many(f, ko, k)
+    tm.consolidate(MAX_P, 1)
+    t_build = time.perf_counter() - t0
+    info = tm.table_info()
+
+    stream = torch.cuda.current_stream()
+    dq = torch.from_numpy(q.view(np.int32)).to("cuda")
+    base = dq.data_ptr()
+    nq = q.shape[0]
+    B = args.batch
+
+    def step():
+        keys = 0
+        for b0 in range(0, nq, B):
+            n = min(B, nq - b0)
+            _, _, nk = tm.match_batch_device(base + b0 * 24, n, unique=args.unique, stream=stream.cuda_stream)
+            keys += nk
+        return keys
+
+    for _ in range(args.warmup):
+        step_keys = step()
+    tm.reset_match_stats()
+    tm.set_profiling(True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step_keys = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    tm.set_profiling(False)
+    ms = e0.elapsed_time(e1) / args.steps
+    ms_max = max_over_ranks(ms, world, device="cuda")
+    st = tm.match_stats()
+    clocks = clk.summary()
+
+    # roofline of the subset-test kernel: algorithmic bytes per launch
+    # (24 B per filter streamed once per 256-query chunk, 24 B per routed
+    # query, 8 B per matching pair) over its event-timed duration
+    launches = max(st["match_kernel_launches"], 1)
+    alg_bytes = (st["dense_tests"] * 24 / 256 + st["routed"] * 24 + st["pairs"] * 8) / launches
+    kern_s = st["match_kernel_ms"] / 1e3 / launches
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / kern_s / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "k_match_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            pj = json.load(fh)
+        # scale the captured small case to a full launch by dense work
+        if pj.get("dense_tests_per_launch"):
+            traffic = pj["dram_bytes_per_launch"] * (st["dense_tests"] / launches) / pj["dense_tests_per_launch"]
+    int_ops = 6 * st["dense_tests"] / launches
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "peak_source": peak_kind,
+                "kernel": "k_match (subset test)", "kernel_ms_per_launch": round(kern_s * 1e3, 3),
+                "alg_bytes_per_launch": int(alg_bytes),
+                "dense_word_tests_per_s": round(int_ops / kern_s / 1e12, 2),
+                "dense_word_tests_unit": "T/s (6 per routed (query, filter) pair, before tile pruning)"}
+
+    line = {"metric": METRIC, "value": round(world * nq / (ms_max / 1e3), 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"config1: {args.filters} filters (seed 2), {nq} queries/step/GPU, "
+                                   f"partitions <= {MAX_P}, 256-query partition batches, "
+                                   f"{'match_unique' if args.unique else 'match'}",
+                       "filters": args.filters, "queries_per_step_per_gpu": nq, "device_batch": B,
+                       "partitions": info["partitions"], "tiles": info["tiles"],
+                       "table_device_bytes": info["device_bytes"],
+                       "l2": "inputs larger than L2 (table %.0f MB + per-step queues and results)" % (
+                           info["device_bytes"] / 2**20),
+                       "parallelism": f"replicas x{world}", "build_s": round(t_build, 2), "gen_s": round(t_gen, 2)},
+            "clocks": clocks, "gpu_launches": int(st["kernel_launches"]), "roofline": roofline,
+            "matches": {"routed_per_query": round(st["routed"] / max(st["queries"], 1), 2),
+                        "pairs_per_query": round(st["pairs"] / max(st["queries"], 1), 2),
+                        "keys_per_query": round(st["keys"] / max(st["queries"], 1), 2)}}
+
+    # ---- end to end through the host C ABI ----
+    if not args.no_e2e:
+        tm.set_batch_limit(B)
+        qh = torch.from_numpy(q.view(np.int32)).pin_memory().numpy().view(np.uint32)
+        need = int(step_keys * 1.05) + 1024
+        try:
+            import psutil
+            avail = psutil.virtual_memory().available
+        except Exception:
+            avail = None
+        e2e_nq = nq
+        if avail is not None and need * 4 > 0.6 * avail:
+            e2e_nq = max(B, int(nq * 0.6 * avail / (need * 4)))
+            need = int(need * e2e_nq / nq) + 1024
+        out_keys = np.empty(need, dtype=np.uint32)
+        out_off = np.empty(e2e_nq + 1, dtype=np.uint64)
+        import ctypes
+
+        from tagmatch_b200 import _native
+        lib = _native.load()
+        nk = ctypes.c_uint64(0)
+
+        def e2e_step():
+            s = lib.tm_match_batch(tm._h, qh[:e2e_nq].ctypes.data_as(_native.u32p), e2e_nq, 1 if args.unique else 0,
+                                   out_off.ctypes.data_as(_native.u64p), out_keys.ctypes.data_as(_native.u32p),
+                                   out_keys.size, ctypes.byref(nk))
+            if s != 0:
+                raise RuntimeError(f"tm_match_batch failed: {s}")
+
+        e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        e2e_steps = max(1, min(args.steps, 3))
+        for _ in range(e2e_steps):
+            e2e_step()
+        dt = (time.perf_counter() - t0) / e2e_steps
+        dt = max_over_ranks(dt, world, device="cuda")
+        line["e2e"] = {"value": round(world * e2e_nq / dt, 1), "unit": UNIT, "h2d_bytes_per_step": e2e_nq * 24,
+                       "d2h_bytes_per_step": int((e2e_nq + 1) * 8 + nk.value * 4), "queries_per_step": e2e_nq,
+                       "api": "tm_match_batch (host buffers, pageable output)"}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(f, ko, k, q, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tm.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    world, rank, local = dist_setup("gloo")
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    from oracle import oracle
+    from tagmatch_b200 import workload
+    if not os.path.exists(oracle.REF_MATCHER):
+        print(json.dumps({"impl": "reference", "metric": METRIC, "unit": UNIT,
+                          "unavailable": "oracle/_ref/test_matcher was not built from the reference sources"}))
+        return
+    f, ko, k = workload.generate_filters(args.filters, SEED)
+    q = workload.generate_queries(max(args.queries, 1), f, SEED)
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        fp = os.path.join(d, "filters.bin")
+        oracle.write_partition_fib(fp, f, ko, k)
+        empty = os.path.join(d, "empty.bin")
+        open(empty, "wb").close()
+
+        def run_shards(per_proc, offset):
+            files = []
+            for c in range(cores):
+                qp = os.path.join(d, f"q{c}.bin")
+                lo = offset + c * per_proc
+                np.ascontiguousarray(q[lo % q.shape[0]:][:per_proc], dtype="<u4").tofile(qp)
+                files.append(qp)
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([oracle.REF_MATCHER, "F=" + fp, "Q=" + qp], stdout=subprocess.DEVNULL)
+                     for qp in files]
+            for p in procs:
+                p.wait()
+            return time.perf_counter() - t0
+
+        # table load time of test_matcher (no queries), subtracted from every step
+        t0 = time.perf_counter()
+        procs = [subprocess.Popen([oracle.REF_MATCHER, "F=" + fp, "Q=" + empty], stdout=subprocess.DEVNULL)
+                 for _ in range(cores)]
+        for p in procs:
+            p.wait()
+        t_load = time.perf_counter() - t0
+        # calibrate queries per process for ~10 s of matching per step
+        per = 2
+        t = run_shards(per, 0) - t_load
+        per = int(max(2, min(4096, per * 10.0 / max(t, 1e-3))))
+        for w in range(args.warmup):
+            run_shards(per, (w + 1) * per * cores)
+        times = []
+        for s in range(args.steps):
+            times.append(max(1e-6, run_shards(per, (args.warmup + s + 1) * per * cores) - t_load))
+    v = per * cores / statistics.mean(times)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 2), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * statistics.mean(times), 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"config1: {args.filters} filters (seed 2), {per * cores} sampled queries/step",
+                       "filters": args.filters},
+            "cpu_baseline": {"value": round(v, 2), "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{per} queries x {cores} test_matcher processes per step; "
+                                       f"table load ({t_load:.1f} s) subtracted"},
+            "e2e": {"value": round(v, 2), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,167 @@
+/*
+ * TagMatch B200 engine: C ABI.
+ *
+ * Subset matching of 192-bit Bloom filters: every stored filter f carries a
+ * set of uint32 keys; a query q returns the keys of every stored f with
+ * f & ~q == 0.  Filters and queries are passed as 6 uint32 words; bit p of
+ * the filter is bit (p % 32) of word p / 32, i.e. the little-endian image of
+ * the reference's 24-byte binary record (bitvector.hh:210-212,
+ * test_io.cc:50-68).
+ *
+ * The reference's interface is the static C++ class in tagmatch.hh:11-37 (a
+ * process-wide singleton).  Here the same operations act on an engine
+ * handle, and each entry point below names the reference member it
+ * replaces.  A C++ facade with the reference's own class and header names
+ * (include/tagmatch/tagmatch.hh) is built on top of these calls.
+ *
+ * Every call returns TM_OK (0) or a negative status; tm_last_error() gives
+ * the message of the last failure on that handle.  No call ends the process
+ * on a CUDA error (the reference prints and exits, gpu.cu:14-24).
+ */
+#ifndef TAGMATCH_B200_H
+#define TAGMATCH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TM_OK 0
+#define TM_ERR_INVALID (-1)  /* bad argument */
+#define TM_ERR_CUDA (-2)     /* CUDA runtime failure */
+#define TM_ERR_STATE (-3)    /* call not valid in the current state */
+#define TM_ERR_CAPACITY (-4) /* output buffer too small; required size reported */
+#define TM_ERR_NOMEM (-5)    /* device or pinned allocation failed */
+#define TM_ERR_IO (-6)       /* database file error */
+#define TM_ERR_TIMEOUT (-7)  /* a bounded device-side wait expired */
+#define TM_ERR_INTERNAL (-8)
+
+#define TM_FILTER_WORDS 6
+
+typedef struct tm_engine tm_engine;
+
+/* Asynchronous completion callback (match_handler::match_done,
+ * match_handler.hh:15-22): called exactly once per request on an engine
+ * thread.  keys is valid only during the call. */
+typedef void (*tm_match_callback)(void *user, uint64_t tag, const uint32_t *keys, uint64_t n_keys);
+
+/* Creates / destroys an engine (the reference's static state).  Device
+ * work starts at the first consolidate on CUDA device 0. */
+int tm_create(tm_engine **out);
+void tm_destroy(tm_engine *e);
+const char *tm_last_error(const tm_engine *e);
+const char *tm_version(void);
+
+/* tagmatch::add(const filter_t &, const std::vector<tagmatch_key_t> &) and
+ * tagmatch::add(const filter_t &, tagmatch_key_t) -- tagmatch.cc:66-77.
+ * Stages keys for a filter until the next consolidate. */
+int tm_add(tm_engine *e, const uint32_t filter[TM_FILTER_WORDS], const uint32_t *keys, uint32_t n_keys);
+/* Bulk form: n filters [n][6] with keys in CSR form (key_offsets[n + 1]). */
+int tm_add_many(tm_engine *e, const uint32_t *filters, uint64_t n, const uint32_t *key_offsets, const uint32_t *keys);
+/* tagmatch::remove(const filter_t &, tagmatch_key_t) -- tagmatch.cc:62-64. */
+int tm_remove(tm_engine *e, const uint32_t filter[TM_FILTER_WORDS], uint32_t key);
+
+/* tagmatch::get/set_database_filename -- tagmatch.hh:22-23, tagmatch.cc:79-87. */
+int tm_set_database_filename(tm_engine *e, const char *name);
+const char *tm_get_database_filename(const tm_engine *e);
+/* Keep the database in memory instead of the file (default: file, as the
+ * reference).  No reference counterpart. */
+int tm_set_persistence(tm_engine *e, int on);
+
+/* tagmatch::consolidate(unsigned partition_size, unsigned threads) --
+ * tagmatch.cc:92-165.  Merges staged updates into the table, rewrites the
+ * database file, runs the GPU partitioner and builds the device table.
+ * threads is kept for interface parity (the partitioner runs on the GPU). */
+int tm_consolidate(tm_engine *e, uint32_t partition_size, uint32_t threads);
+/* tagmatch::consolidate() with the stored parameters (default 1000, 1). */
+int tm_consolidate_default(tm_engine *e);
+
+/* tagmatch::start(unsigned threads, unsigned gpu_count) -- tagmatch.cc:179-186.
+ * Replicates the table on gpu_count devices and starts the asynchronous
+ * matcher.  Re-entrant. */
+int tm_start(tm_engine *e, uint32_t threads, uint32_t gpu_count);
+/* tagmatch::stop() -- tagmatch.cc:188-191, front_end.cc:693-771.  Flushes
+ * every pending asynchronous request (all callbacks have fired on return).
+ * Re-entrant. */
+int tm_stop(tm_engine *e);
+/* tagmatch::clear() -- tagmatch.cc:193-198. */
+int tm_clear(tm_engine *e);
+/* tagmatch::get/set_latency_limit_ms -- tagmatch.cc:166-168,
+ * front_end.cc:555-561: a pending asynchronous batch older than this is
+ * flushed; 0 means batches go out only when full or at stop(). */
+int tm_set_latency_limit_ms(tm_engine *e, uint32_t ms);
+uint32_t tm_get_latency_limit_ms(const tm_engine *e);
+/* Largest number of queries per device batch (default 65536). */
+int tm_set_batch_limit(tm_engine *e, uint32_t queries);
+
+/* tagmatch::match / tagmatch::match_unique (tagmatch.cc:200-210) for a
+ * whole batch, synchronously.  queries: n [n][6] words.  out_offsets:
+ * n + 1 entries; the keys of query i are out_keys[out_offsets[i] ..
+ * out_offsets[i + 1]).  unique = 0: every key of every matching filter
+ * (test_matcher.cc:74-81 order is not kept; the multiset is); unique != 0:
+ * each query's keys sorted ascending without duplicates
+ * (tagmatch_query.hh:99-119).  If capacity is too small, returns
+ * TM_ERR_CAPACITY with the required key count in *n_keys (offsets are
+ * complete).  Requires a consolidated table. */
+int tm_match_batch(tm_engine *e, const uint32_t *queries, uint64_t n, int unique, uint64_t *out_offsets,
+                   uint32_t *out_keys, uint64_t capacity, uint64_t *n_keys);
+
+/* Device-resident form on CUDA device 0: queries, results and stream are
+ * device objects.  *d_offsets / *d_keys point into engine-owned device
+ * memory valid until the next match call on this engine. */
+int tm_match_batch_device(tm_engine *e, const uint32_t *d_queries, uint32_t n, int unique, const uint64_t **d_offsets,
+                          const uint32_t **d_keys, uint64_t *n_keys, void *stream);
+
+/* tagmatch::match / match_unique with a handler (tagmatch.cc:200-210,
+ * front_end.cc:540-551): queues one query; cb(user, tag, keys, n) fires
+ * once, on an engine thread, after the query's batch completes. */
+int tm_match_async(tm_engine *e, const uint32_t query[TM_FILTER_WORDS], int unique, uint64_t tag, tm_match_callback cb,
+                   void *user);
+
+/* partitioning::balanced_partitioning(fib, masks) -- partitioning.cc:361-411,
+ * run by the GPU partitioner.  filters: n unique filters [n][6].
+ * partition_of[i] receives filter i's partition id; masks[p][6] the AND of
+ * partition p's members (all ones for an empty partition); sizes[p] its
+ * member count.  Partition ids follow the filters' position after the
+ * splits.  Returns TM_ERR_CAPACITY with the count in *n_partitions when
+ * capacity partitions do not fit. */
+int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p, uint32_t *partition_of,
+                             uint32_t *masks, uint32_t *sizes, uint64_t capacity, uint64_t *n_partitions);
+
+/* Table statistics after consolidate. */
+typedef struct {
+    uint64_t filters;
+    uint64_t keys;
+    uint64_t partitions;
+    uint64_t tiles;
+    uint64_t device_bytes;
+    uint32_t max_key;
+} tm_table_info;
+int tm_get_table_info(tm_engine *e, tm_table_info *info);
+
+/* Cumulative statistics of the synchronous matcher: batches, queries,
+ * routed (query, partition) pairs, work items, matching (query, filter)
+ * pairs, output keys, pair-buffer regrowths; with profiling on, the
+ * subset-test kernel's launches and total time from CUDA events recorded
+ * on its stream.  No reference counterpart (front_end::print_statistics,
+ * front_end.cc:781-789, is the closest). */
+typedef struct {
+    uint64_t batches, queries, routed, items, pairs, keys;
+    uint64_t pair_retries;
+    uint64_t match_kernel_launches;
+    double match_kernel_ms;
+    uint64_t dense_tests; /* sum over batches and partitions of routed queries x partition size */
+    uint64_t kernel_launches; /* all kernels launched by the matcher */
+} tm_match_stats;
+int tm_get_match_stats(tm_engine *e, tm_match_stats *st);
+int tm_reset_match_stats(tm_engine *e);
+/* Turns CUDA-event timing of the subset-test kernel on or off. */
+int tm_set_profiling(tm_engine *e, int on);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TAGMATCH_B200_H */

@@ -1,0 +1,401 @@
+// TagMatch engine implementation.
+#include "engine.cuh"
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+
+namespace tmb {
+
+void KeysetChange::apply(std::vector<uint32_t> &keys) const {
+    std::vector<uint32_t> out;
+    out.reserve(keys.size() + to_add.size());
+    std::set<uint32_t> adds = to_add;
+    for (uint32_t k : keys) {
+        adds.erase(k);
+        if (to_remove.count(k)) continue;
+        out.push_back(k);
+    }
+    for (uint32_t k : adds) out.push_back(k);
+    keys.swap(out);
+}
+
+Engine::Engine() {}
+
+Engine::~Engine() {
+    try {
+        stop();
+    } catch (...) {
+    }
+    for (auto &d : devs_) {
+        if (d && d->stream) {
+            cudaSetDevice(d->id);
+            cudaStreamDestroy(d->stream);
+        }
+    }
+}
+
+void Engine::add(const uint32_t *filter, const uint32_t *keys, uint32_t n) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    FilterKey f;
+    std::memcpy(f.w.data(), filter, sizeof(f.w));
+    KeysetChange &c = updates_[f];
+    for (uint32_t i = 0; i < n; ++i) c.to_add.insert(keys[i]);
+}
+
+void Engine::remove(const uint32_t *filter, uint32_t key) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    FilterKey f;
+    std::memcpy(f.w.data(), filter, sizeof(f.w));
+    updates_[f].to_remove.insert(key);
+}
+
+namespace {
+
+struct Entry {
+    FilterKey f;
+    std::vector<uint32_t> keys;
+};
+
+// The reference writes each database record as a partition_fib_entry
+// (tagmatch.cc:132-142 -> fib.hh:46-49): uint32 partition id, the 24-byte
+// filter, uint32 key count, the keys (fib.cc:14-21).  Records are read back
+// in that same layout.  (The reference reads them as plain fib_entry,
+// tagmatch.cc:101-106, one field short.)
+bool read_db(const std::string &fn, std::vector<Entry> &out, std::map<FilterKey, KeysetChange> &updates) {
+    std::ifstream in(fn, std::ios::binary);
+    if (!in) return false;
+    for (;;) {
+        uint32_t part, n;
+        Entry e;
+        if (!in.read(reinterpret_cast<char *>(&part), 4)) break;
+        if (!in.read(reinterpret_cast<char *>(e.f.w.data()), 24)) break;
+        if (!in.read(reinterpret_cast<char *>(&n), 4)) break;
+        e.keys.resize(n);
+        if (n && !in.read(reinterpret_cast<char *>(e.keys.data()), std::streamsize(n) * 4)) break;
+        auto it = updates.find(e.f);
+        if (it != updates.end()) {
+            it->second.apply(e.keys);
+            updates.erase(it);
+        }
+        if (!e.keys.empty()) out.push_back(std::move(e));
+    }
+    return true;
+}
+
+bool write_db(const std::string &fn, const std::vector<Entry> &fib) {
+    std::ofstream out(fn, std::ios::binary | std::ios::trunc);
+    if (!out) return false;
+    const uint32_t part = 0;
+    for (const Entry &e : fib) {
+        const uint32_t n = uint32_t(e.keys.size());
+        out.write(reinterpret_cast<const char *>(&part), 4);
+        out.write(reinterpret_cast<const char *>(e.f.w.data()), 24);
+        out.write(reinterpret_cast<const char *>(&n), 4);
+        if (n) out.write(reinterpret_cast<const char *>(e.keys.data()), std::streamsize(n) * 4);
+    }
+    return bool(out);
+}
+
+}  // namespace
+
+void Engine::consolidate(uint32_t psize, uint32_t threads) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (psize == 0) throw Error(TM_ERR_INVALID, "partition size must be at least 1");
+    if (started_) throw Error(TM_ERR_STATE, "consolidate() while matching: call stop() first");
+    partition_size_ = psize;
+    partitioning_threads_ = threads;
+    std::vector<Entry> fib;
+    if (already_consolidated_) {
+        if (persist_) {
+            if (!read_db(db_filename_, fib, updates_))
+                std::cerr << "could not open database file: " << db_filename_ << std::endl;
+        } else {
+            // in-memory database: the current table
+            const uint32_t n = n_filters();
+            for (uint32_t i = 0; i < n; ++i) {
+                Entry e;
+                std::memcpy(e.f.w.data(), &filters_[size_t(i) * kWords], 24);
+                e.keys.assign(keys_.begin() + key_off_[i], keys_.begin() + key_off_[i + 1]);
+                auto it = updates_.find(e.f);
+                if (it != updates_.end()) {
+                    it->second.apply(e.keys);
+                    updates_.erase(it);
+                }
+                if (!e.keys.empty()) fib.push_back(std::move(e));
+            }
+        }
+    }
+    for (auto &u : updates_) {
+        Entry e;
+        e.f = u.first;
+        u.second.apply(e.keys);
+        if (!e.keys.empty()) fib.push_back(std::move(e));
+    }
+    updates_.clear();
+    if (persist_ && !write_db(db_filename_, fib))
+        std::cerr << "could not open database file: " << db_filename_ << std::endl;
+
+    uint64_t nk = 0;
+    for (const Entry &e : fib) nk += e.keys.size();
+    if (nk >= 0xFFFFFFFFull || fib.size() >= 0xFFFFFFFFull) throw Error(TM_ERR_INVALID, "table too large (2^32 keys or filters)");
+    filters_.resize(fib.size() * kWords);
+    key_off_.assign(fib.size() + 1, 0);
+    keys_.clear();
+    keys_.reserve(nk);
+    for (size_t i = 0; i < fib.size(); ++i) {
+        std::memcpy(&filters_[i * kWords], fib[i].f.w.data(), 24);
+        keys_.insert(keys_.end(), fib[i].keys.begin(), fib[i].keys.end());
+        key_off_[i + 1] = uint32_t(keys_.size());
+    }
+    ++table_version_;
+    // the partitioner runs at consolidation time, on the first device
+    build_device_table(device(0));
+    already_consolidated_ = true;
+}
+
+Engine::Device &Engine::device(int i) {
+    while ((int)devs_.size() <= i) {
+        auto d = std::make_unique<Device>();
+        d->id = int(devs_.size());
+        TM_CUDA(cudaSetDevice(d->id));
+        TM_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+        devs_.push_back(std::move(d));
+        dev_version_.push_back(~0ull);
+    }
+    return *devs_[i];
+}
+
+void Engine::build_device_table(Device &d) {
+    TM_CUDA(cudaSetDevice(d.id));
+    const uint32_t n = n_filters();
+    DevBuf<uint32_t> f, ko, k;
+    f.reserve(size_t(n) * kWords);
+    ko.reserve(size_t(n) + 1);
+    k.reserve(std::max<size_t>(keys_.size(), 1));
+    if (n) {
+        TM_CUDA(cudaMemcpyAsync(f.p, filters_.data(), filters_.size() * 4, cudaMemcpyHostToDevice, d.stream));
+        TM_CUDA(cudaMemcpyAsync(ko.p, key_off_.data(), key_off_.size() * 4, cudaMemcpyHostToDevice, d.stream));
+        if (!keys_.empty()) TM_CUDA(cudaMemcpyAsync(k.p, keys_.data(), keys_.size() * 4, cudaMemcpyHostToDevice, d.stream));
+    }
+    PartitionResult pr;
+    gpu_partition(f.p, n, partition_size_, true, pr, d.stream);
+    d.table = DevTable();
+    build_table(pr, ko.p, k.p, keys_.size(), d.table, d.stream);
+    TM_CUDA(cudaStreamSynchronize(d.stream));
+    d.table_ready = true;
+    dev_version_[d.id] = table_version_;
+}
+
+uint32_t Engine::n_partitions() const { return devs_.empty() ? 0 : devs_[0]->table.n_parts; }
+uint32_t Engine::n_tiles() const { return devs_.empty() ? 0 : devs_[0]->table.n_tiles; }
+size_t Engine::device_bytes() const { return devs_.empty() ? 0 : devs_[0]->table.device_bytes(); }
+const DevTable *Engine::table(int dev) const {
+    return dev < (int)devs_.size() && devs_[dev]->table_ready ? &devs_[dev]->table : nullptr;
+}
+
+void Engine::start(uint32_t threads, uint32_t gpus) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (gpus == 0) gpus = 1;
+    int count = 0;
+    TM_CUDA(cudaGetDeviceCount(&count));
+    if ((int)gpus > count) throw Error(TM_ERR_INVALID, "start(): " + std::to_string(gpus) + " GPUs requested, " +
+                                                            std::to_string(count) + " present");
+    threads_ = threads;
+    if (started_) return;  // re-entrant, like front_end::start (front_end.cc:671-691)
+    gpus_ = gpus;
+    for (uint32_t g = 0; g < gpus_; ++g) {
+        Device &d = device(int(g));
+        if (dev_version_[g] != table_version_) build_device_table(d);  // replicas (back_end.cc:444-447)
+    }
+    {
+        std::lock_guard<std::mutex> ql(q_mtx_);
+        started_ = true;
+        stopping_ = false;
+        flush_now_ = false;
+        if (!pending_.empty()) oldest_ = std::chrono::steady_clock::now();
+    }
+    for (uint32_t g = 0; g < gpus_; ++g) devs_[g]->worker = std::thread(&Engine::worker_loop, this, int(g));
+}
+
+void Engine::stop() {
+    {
+        std::lock_guard<std::mutex> ql(q_mtx_);
+        if (!started_ || stopping_) return;
+        stopping_ = true;
+    }
+    q_cv_.notify_all();
+    for (auto &d : devs_)
+        if (d->worker.joinable()) d->worker.join();
+    std::lock_guard<std::mutex> ql(q_mtx_);
+    started_ = false;
+    stopping_ = false;
+    flush_now_ = false;
+}
+
+void Engine::clear() {
+    stop();
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    already_consolidated_ = false;
+    updates_.clear();
+    filters_.clear();
+    key_off_.assign(1, 0);
+    keys_.clear();
+    ++table_version_;
+    for (auto &d : devs_) {
+        TM_CUDA(cudaSetDevice(d->id));
+        d->table = DevTable();
+        d->scratch = MatchScratch();
+        d->table_ready = false;
+    }
+}
+
+void Engine::submit(const AsyncRequest &r) {
+    {
+        std::lock_guard<std::mutex> ql(q_mtx_);
+        if (pending_.empty()) oldest_ = std::chrono::steady_clock::now();
+        pending_.push_back(r);
+    }
+    q_cv_.notify_one();
+}
+
+void Engine::worker_loop(int dev) {
+    Device &d = *devs_[dev];
+    cudaSetDevice(d.id);
+    std::vector<AsyncRequest> batch;
+    for (;;) {
+        batch.clear();
+        {
+            std::unique_lock<std::mutex> lk(q_mtx_);
+            for (;;) {
+                if (!pending_.empty()) {
+                    if (stopping_ || flush_now_ || pending_.size() >= batch_limit_) break;
+                    const uint32_t lim = latency_ms_.load();
+                    if (lim > 0) {
+                        auto due = oldest_ + std::chrono::milliseconds(lim);
+                        if (std::chrono::steady_clock::now() >= due) break;
+                        q_cv_.wait_until(lk, due);
+                        continue;
+                    }
+                } else if (stopping_) {
+                    return;
+                }
+                q_cv_.wait(lk);
+            }
+            const size_t take = std::min<size_t>(pending_.size(), batch_limit_);
+            for (size_t i = 0; i < take; ++i) {
+                batch.push_back(pending_.front());
+                pending_.pop_front();
+            }
+            if (!pending_.empty()) oldest_ = std::chrono::steady_clock::now();
+            in_flight_ += batch.size();
+        }
+        run_async_batch(d, batch);
+        {
+            std::lock_guard<std::mutex> lk(q_mtx_);
+            in_flight_ -= batch.size();
+        }
+        done_cv_.notify_all();
+    }
+}
+
+void Engine::run_async_batch(Device &d, std::vector<AsyncRequest> &batch) {
+    // match and match_unique requests of one batch run as two sub-batches
+    for (int u = 0; u < 2; ++u) {
+        std::vector<size_t> idx;
+        for (size_t i = 0; i < batch.size(); ++i)
+            if (batch[i].unique == (u == 1)) idx.push_back(i);
+        if (idx.empty()) continue;
+        const uint32_t nq = uint32_t(idx.size());
+        bool ok = true;
+        try {
+            d.h_queries.reserve(size_t(nq) * kWords);
+            for (uint32_t i = 0; i < nq; ++i) std::memcpy(d.h_queries.p + size_t(i) * kWords, batch[idx[i]].words, 24);
+            d.scratch.queries.reserve(size_t(nq) * kWords);
+            TM_CUDA(cudaMemcpyAsync(d.scratch.queries.p, d.h_queries.p, size_t(nq) * 24, cudaMemcpyHostToDevice, d.stream));
+            const uint64_t *doff;
+            const uint32_t *dkeys;
+            uint64_t nk = 0;
+            BatchStats bs;
+            match_batch(d.table, d.scratch.queries.p, nq, u == 1, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
+            d.h_offsets.reserve(size_t(nq) + 1);
+            d.h_keys.reserve(std::max<uint64_t>(nk, 1));
+            TM_CUDA(cudaMemcpyAsync(d.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, d.stream));
+            if (nk) TM_CUDA(cudaMemcpyAsync(d.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, d.stream));
+            TM_CUDA(cudaStreamSynchronize(d.stream));
+        } catch (const Error &e) {
+            ok = false;
+            std::lock_guard<std::mutex> lk(q_mtx_);
+            async_error_ = e.what();
+        }
+        for (uint32_t i = 0; i < nq; ++i) {
+            const AsyncRequest &r = batch[idx[i]];
+            if (!r.cb) continue;
+            if (ok) {
+                const uint64_t b = d.h_offsets.p[i], e = d.h_offsets.p[i + 1];
+                r.cb(r.user, r.tag, d.h_keys.p + b, e - b);
+            } else {
+                r.cb(r.user, r.tag, nullptr, 0);
+            }
+        }
+    }
+}
+
+void Engine::match_device(const uint32_t *d_queries, uint32_t nq, bool unique, const uint64_t **d_offsets,
+                          const uint32_t **d_keys, uint64_t *n_keys, cudaStream_t st, BatchStats *bs, cudaEvent_t ev0,
+                          cudaEvent_t ev1) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (!already_consolidated_) throw Error(TM_ERR_STATE, "match before consolidate()");
+    Device &d = device(0);
+    if (dev_version_[0] != table_version_) build_device_table(d);
+    TM_CUDA(cudaSetDevice(d.id));
+    BatchStats local;
+    d.scratch.profile = profile_;
+    match_batch(d.table, d_queries, nq, unique, d.scratch, d_offsets, d_keys, n_keys, &local, st ? st : d.stream, ev0, ev1);
+    stats_.add(local, nq, profile_);
+    if (bs) *bs = local;
+}
+
+void Engine::set_profiling(bool on) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    profile_ = on;
+}
+
+void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
+                        uint64_t capacity, uint64_t *n_keys) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (!already_consolidated_) throw Error(TM_ERR_STATE, "match before consolidate()");
+    Device &d = device(0);
+    if (dev_version_[0] != table_version_) build_device_table(d);
+    TM_CUDA(cudaSetDevice(d.id));
+    uint64_t total = 0;
+    bool overflow = false;
+    out_offsets[0] = 0;
+    for (uint64_t q0 = 0; q0 < nq; q0 += batch_limit_) {
+        const uint32_t n = uint32_t(std::min<uint64_t>(batch_limit_, nq - q0));
+        d.scratch.queries.reserve(size_t(n) * kWords);
+        TM_CUDA(cudaMemcpyAsync(d.scratch.queries.p, queries + q0 * kWords, size_t(n) * 24, cudaMemcpyHostToDevice, d.stream));
+        const uint64_t *doff;
+        const uint32_t *dkeys;
+        uint64_t nk = 0;
+        BatchStats bs;
+        d.scratch.profile = profile_;
+        match_batch(d.table, d.scratch.queries.p, n, unique, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
+        stats_.add(bs, n, profile_);
+        TM_CUDA(cudaMemcpyAsync(out_offsets + q0 + 1, doff + 1, size_t(n) * 8, cudaMemcpyDeviceToHost, d.stream));
+        if (!overflow && total + nk <= capacity) {
+            if (nk) TM_CUDA(cudaMemcpyAsync(out_keys + total, dkeys, nk * 4, cudaMemcpyDeviceToHost, d.stream));
+        } else {
+            overflow = true;
+        }
+        TM_CUDA(cudaStreamSynchronize(d.stream));
+        for (uint32_t i = 1; i <= n; ++i) out_offsets[q0 + i] += total;
+        total += nk;
+    }
+    *n_keys = total;
+    if (overflow) throw Error(TM_ERR_CAPACITY, "output key buffer too small: " + std::to_string(total) + " keys needed");
+}
+
+}  // namespace tmb

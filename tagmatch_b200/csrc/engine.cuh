@@ -1,0 +1,180 @@
+// TagMatch engine: update staging, consolidation (GPU partitioner + device
+// table), batched and asynchronous matching on one or more devices.
+#pragma once
+#include <array>
+#include <atomic>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <thread>
+#include <vector>
+#include "match.cuh"
+
+namespace tmb {
+
+// 192-bit filter as 6 words, ordered like bitvector<192>::operator<
+// (bitvector.hh:389-397): the lowest differing bit of the first differing
+// 64-bit block decides, the side holding a 1 is greater.
+struct FilterKey {
+    std::array<uint32_t, kWords> w;
+    bool operator<(const FilterKey &o) const {
+        for (int blk = 0; blk < 3; ++blk) {
+            const uint64_t x = uint64_t(w[2 * blk]) | (uint64_t(w[2 * blk + 1]) << 32);
+            const uint64_t y = uint64_t(o.w[2 * blk]) | (uint64_t(o.w[2 * blk + 1]) << 32);
+            if (x != y) return (y >> __builtin_ctzll(x ^ y)) & 1;
+        }
+        return false;
+    }
+    bool operator==(const FilterKey &o) const { return w == o.w; }
+};
+
+// Pending key additions/removals for one filter (tagmatch.cc:22-34).
+struct KeysetChange {
+    std::set<uint32_t> to_add, to_remove;
+    // Applies the change to an existing key vector: removed keys go, kept
+    // keys keep their order, new keys follow in ascending order.  (The
+    // reference's apply, tagmatch.cc:36-59, never shrinks the vector, so a
+    // removal there only sticks when enough keys are added in the same
+    // update; here removals always take effect.)
+    void apply(std::vector<uint32_t> &keys) const;
+};
+
+typedef void (*MatchCallback)(void *user, uint64_t tag, const uint32_t *keys, uint64_t n_keys);
+
+struct AsyncRequest {
+    uint32_t words[kWords];
+    bool unique;
+    uint64_t tag;
+    MatchCallback cb;
+    void *user;
+};
+
+struct EngineStats {
+    uint64_t batches = 0, queries = 0, routed = 0, items = 0, pairs = 0, keys = 0;
+    uint64_t pair_retries = 0;
+    uint64_t match_launches = 0;
+    double match_ms = 0.0;
+    uint64_t dense = 0, launches = 0;
+    void add(const BatchStats &b, uint32_t nq, bool profiled) {
+        batches++;
+        queries += nq;
+        routed += b.routed;
+        items += b.items;
+        pairs += b.pairs;
+        keys += b.keys;
+        pair_retries += b.retries;
+        dense += b.dense;
+        launches += b.launches;
+        if (profiled) {
+            match_launches += 1 + b.retries;
+            match_ms += b.match_ms;
+        }
+    }
+};
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+
+    // staging (tagmatch.cc:62-77)
+    void add(const uint32_t *filter, const uint32_t *keys, uint32_t n);
+    void remove(const uint32_t *filter, uint32_t key);
+    void set_db(const std::string &f) { db_filename_ = f; }
+    const std::string &db() const { return db_filename_; }
+    void set_persist(bool on) { persist_ = on; }
+
+    // tagmatch.cc:92-165
+    void consolidate(uint32_t partition_size, uint32_t threads);
+    void consolidate() { consolidate(partition_size_, partitioning_threads_); }
+
+    // tagmatch.cc:174-198
+    void start(uint32_t threads, uint32_t gpus);
+    void start() { start(threads_, gpus_); }
+    void stop();
+    void clear();
+    void set_latency_limit_ms(uint32_t ms) { latency_ms_.store(ms); }
+    uint32_t latency_limit_ms() const { return latency_ms_.load(); }
+    void set_batch_limit(uint32_t q) { batch_limit_ = q ? q : 1; }
+
+    // synchronous batch match with host buffers; returns TM_ERR_CAPACITY
+    // through the exception when out_keys is too small (needed in *n_keys)
+    void match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
+                    uint64_t capacity, uint64_t *n_keys);
+    // synchronous batch match with device buffers on device 0
+    void match_device(const uint32_t *d_queries, uint32_t nq, bool unique, const uint64_t **d_offsets,
+                      const uint32_t **d_keys, uint64_t *n_keys, cudaStream_t st, BatchStats *bs, cudaEvent_t ev0,
+                      cudaEvent_t ev1);
+    // asynchronous match: cb fires exactly once per request, on an engine
+    // thread, after start() (requests made earlier wait for it)
+    void submit(const AsyncRequest &r);
+
+    // table introspection
+    uint32_t n_filters() const { return uint32_t(key_off_.size() ? key_off_.size() - 1 : 0); }
+    uint32_t n_partitions() const;
+    uint32_t n_tiles() const;
+    size_t device_bytes() const;
+    const DevTable *table(int dev = 0) const;
+    const EngineStats &stats() const { return stats_; }
+    void reset_stats() { stats_ = EngineStats(); }
+    void set_profiling(bool on);
+    bool profiling() const { return profile_; }
+    bool started() const { return started_; }
+    // host copy of the consolidated filters (table order) and keys
+    const std::vector<uint32_t> &filters() const { return filters_; }
+    const std::vector<uint32_t> &key_offsets() const { return key_off_; }
+    const std::vector<uint32_t> &keys() const { return keys_; }
+
+private:
+    struct Device {
+        int id = 0;
+        cudaStream_t stream = nullptr;
+        DevTable table;
+        MatchScratch scratch;
+        bool table_ready = false;
+        HostBuf<uint32_t> h_queries;
+        HostBuf<uint64_t> h_offsets;
+        HostBuf<uint32_t> h_keys;
+        std::thread worker;
+    };
+    void build_device_table(Device &d);
+    Device &device(int i);
+    void worker_loop(int dev);
+    void run_async_batch(Device &d, std::vector<AsyncRequest> &batch);
+
+    std::map<FilterKey, KeysetChange> updates_;
+    bool already_consolidated_ = false;
+    bool persist_ = true;
+    std::string db_filename_ = "tagmatch.db";
+    uint32_t partition_size_ = 1000;       // tagmatch.cc:89
+    uint32_t partitioning_threads_ = 1;    // tagmatch.cc:90
+    uint32_t threads_ = 4, gpus_ = 1;      // tagmatch.cc:170-171
+    std::atomic<uint32_t> latency_ms_{0};
+    uint32_t batch_limit_ = 65536;
+
+    // consolidated table on the host, in table order
+    std::vector<uint32_t> filters_, key_off_{0}, keys_;
+    uint64_t table_version_ = 0;
+
+    std::vector<std::unique_ptr<Device>> devs_;
+    std::vector<uint64_t> dev_version_;
+    std::mutex api_mtx_;  // serialises synchronous calls
+    EngineStats stats_;
+    bool profile_ = false;
+
+    // async path
+    std::mutex q_mtx_;
+    std::condition_variable q_cv_, done_cv_;
+    std::deque<AsyncRequest> pending_;
+    std::chrono::steady_clock::time_point oldest_;
+    uint64_t in_flight_ = 0;
+    bool started_ = false, stopping_ = false, flush_now_ = false;
+    std::string async_error_;
+};
+
+}  // namespace tmb

@@ -1,0 +1,63 @@
+// Batched matching on one device: routing, per-partition queues, the
+// subset-test kernel, key gather and match_unique de-duplication.
+#pragma once
+#include <cstdint>
+#include "partition.cuh"
+
+namespace tmb {
+
+constexpr int kSegTiles = 128;  // tiles per work item
+
+// Device scratch for one in-flight batch (grow-only).
+struct MatchScratch {
+    DevBuf<uint32_t> queries;     // [nq][6] staged host input
+    DevBuf<uint32_t> part_count;  // [P]
+    DevBuf<uint32_t> part_off;    // [P + 1]
+    DevBuf<uint32_t> part_cursor; // [P]
+    DevBuf<uint32_t> queue;       // [routed][8]
+    DevBuf<uint32_t> item_count;  // [P]
+    DevBuf<uint32_t> item_off;    // [P + 1]
+    DevBuf<unsigned long long> counters;  // [0] work item, [1] pairs, [2] error flags
+    DevBuf<Pair> pairs;
+    DevBuf<uint32_t> qkeys;       // [nq]
+    DevBuf<uint64_t> qoff;        // [nq + 1]
+    DevBuf<uint32_t> qcursor;     // [nq]
+    DevBuf<uint32_t> keys;        // [total keys] grouped by query
+    DevBuf<uint32_t> ucount;      // [nq]
+    DevBuf<uint64_t> uoff;        // [nq + 1]
+    DevBuf<uint32_t> ukeys;       // [total unique] (also radix temp)
+    std::vector<uint32_t> h_part_count;
+    ScanScratch scr;
+    int sm_count = 0;
+    size_t pair_cap_hint = 0;
+    // optional CUDA-event timing of the subset-test kernel
+    bool profile = false;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    MatchScratch() = default;
+    MatchScratch(const MatchScratch &) = delete;
+    MatchScratch &operator=(const MatchScratch &) = delete;
+    MatchScratch &operator=(MatchScratch &&o) noexcept;
+    ~MatchScratch();
+};
+
+// Per-batch statistics (for the bench and the scheduler).
+struct BatchStats {
+    uint64_t routed = 0;   // (query, partition) pairs
+    uint64_t items = 0;    // work items
+    uint64_t pairs = 0;    // matching (query, filter) pairs
+    uint64_t keys = 0;     // output keys
+    int retries = 0;       // pair-buffer regrowths
+    float match_ms = 0.f;  // subset-test kernel time (profiling on)
+    uint64_t dense = 0;    // sum over partitions of routed queries x partition size
+    uint32_t launches = 0; // kernels launched for the batch
+};
+
+// Matches nq queries already on the device (d_queries [nq][6]).  On return
+// (stream synchronized) *d_offsets points to nq + 1 offsets and *d_keys to
+// the keys of every query, both in scratch memory.  unique != 0 gives each
+// query's keys sorted ascending without duplicates (match_unique).
+void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, MatchScratch &s,
+                 const uint64_t **d_offsets, const uint32_t **d_keys, uint64_t *n_keys, BatchStats *stats,
+                 cudaStream_t st, cudaEvent_t match_begin = nullptr, cudaEvent_t match_end = nullptr);
+
+}  // namespace tmb

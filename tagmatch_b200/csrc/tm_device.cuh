@@ -1,0 +1,55 @@
+// Shared device-side definitions for the TagMatch B200 engine.
+//
+// Filters and queries are 192-bit Bloom filters held as 6 x uint32 words in
+// the reference's 32-bit view (bitvector.hh:210-212): bit p is bit (p % 32)
+// of word p / 32.  f matches q when f is a subset of q, f & ~q == 0
+// (bitvector.hh:282-296).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace tmb {
+
+constexpr int kWords = 6;          // 32-bit words per filter
+constexpr int kBits = 192;         // filter width
+constexpr int kTile = 32;          // filters per tile (one per lane of a warp)
+constexpr int kChunk = 256;        // queries per partition batch (QUERIES_BATCH_SIZE, parameters.hh:13)
+constexpr int kQueueWords = 8;     // queued query record: 6 filter words, query id, pad (32 bytes)
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Tile descriptor: AND of the tile's filters (the bits every member has),
+// member count and owning partition; 32 bytes.
+struct __align__(16) TileInfo {
+    uint32_t and_mask[kWords];
+    uint32_t count;
+    uint32_t partition;
+};
+
+// Matched (query, filter-slot) pair.
+struct __align__(8) Pair {
+    uint32_t query;
+    uint32_t slot;
+};
+
+__device__ __forceinline__ uint32_t andnot_or(uint32_t f, uint32_t q, uint32_t acc) {
+    return (f & ~q) | acc;  // one LOP3
+}
+
+__device__ __forceinline__ bool subset6(const uint32_t *f, const uint32_t *q) {
+    uint32_t a = f[0] & ~q[0];
+    a = andnot_or(f[1], q[1], a);
+    a = andnot_or(f[2], q[2], a);
+    a = andnot_or(f[3], q[3], a);
+    a = andnot_or(f[4], q[4], a);
+    a = andnot_or(f[5], q[5], a);
+    return a == 0;
+}
+
+__device__ __forceinline__ int bit_of(const uint32_t *f, unsigned b) {
+    return (f[b >> 5] >> (b & 31)) & 1;
+}
+
+}  // namespace tmb
+
+// Status codes (TM_OK, TM_ERR_*) come from the C ABI header.
+#include "../../include/tagmatch_b200.h"

@@ -1,0 +1,104 @@
+// Host-side helpers: CUDA error handling and grow-only device buffers.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace tmb {
+
+// Raised inside the engine; the C ABI turns it into a status code and a
+// message (tm_last_error), so no CUDA failure ends the process.
+struct Error : std::runtime_error {
+    int status;
+    Error(int st, const std::string &msg) : std::runtime_error(msg), status(st) {}
+};
+
+inline std::string cuda_msg(cudaError_t e, const char *what, const char *file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    return buf;
+}
+
+#define TM_CUDA(x)                                                                       \
+    do {                                                                                 \
+        cudaError_t e_ = (x);                                                            \
+        if (e_ != cudaSuccess) throw ::tmb::Error(-2, ::tmb::cuda_msg(e_, #x, __FILE__, __LINE__)); \
+    } while (0)
+
+#define TM_CHECK_LAUNCH() TM_CUDA(cudaGetLastError())
+
+// Grow-only device buffer.  reserve() keeps the old contents only when it
+// does not reallocate; callers treat a grown buffer as uninitialised.
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), cap(o.cap) { o.p = nullptr; o.cap = 0; }
+    DevBuf &operator=(DevBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            cap = o.cap;
+            o.p = nullptr;
+            o.cap = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void reserve(size_t n) {
+        if (n <= cap && p) return;
+        release();
+        size_t bytes = (n ? n : 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cap = 0;
+            cudaGetLastError();
+            throw Error(-5, cuda_msg(e, "cudaMalloc", __FILE__, __LINE__) + " bytes=" + std::to_string(bytes));
+        }
+        cap = n ? n : 1;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    T *get() const { return p; }
+};
+
+// Pinned host buffer (grow-only).
+template <class T>
+struct HostBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf &) = delete;
+    HostBuf &operator=(const HostBuf &) = delete;
+    HostBuf(HostBuf &&o) noexcept : p(o.p), cap(o.cap) { o.p = nullptr; o.cap = 0; }
+    ~HostBuf() { release(); }
+    void reserve(size_t n) {
+        if (n <= cap && p) return;
+        release();
+        size_t bytes = (n ? n : 1) * sizeof(T);
+        cudaError_t e = cudaMallocHost(&p, bytes);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            cap = 0;
+            cudaGetLastError();
+            throw Error(-5, cuda_msg(e, "cudaMallocHost", __FILE__, __LINE__));
+        }
+        cap = n ? n : 1;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace tmb

@@ -1,0 +1,272 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and with the
+reference's own outputs.  Bit-exact: same multiset of keys per query for
+match, same sorted unique keys for match_unique."""
+import os
+import subprocess
+import threading
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from tagmatch_b200 import TagMatch, TagMatchError, balanced_partitioning, build, workload
+from tagmatch_b200 import _native
+from tagmatch_b200.tagmatch import filter_from_bits, filter_from_string
+from tests.conftest import golden
+from tests.helpers import assert_same_multisets, groups_from_assignment, load_partitions_golden, read_fixtures
+
+pytestmark = pytest.mark.gpu
+
+
+def engine_with(filters, key_off, keys, max_p=65536):
+    tm = TagMatch()
+    tm.set_persistence(False)
+    tm.add_many(filters, key_off, keys)
+    tm.consolidate(max_p, 1)
+    return tm
+
+
+def check_against_oracle(f, ko, k, q, max_p, unique_too=True):
+    tm = engine_with(f, ko, k, max_p)
+    off, keys = tm.match_batch(q)
+    ooff, okeys = oracle.match(f, ko, k, q)
+    assert_same_multisets(off, keys, ooff, okeys)
+    if unique_too:
+        uoff, ukeys = tm.match_batch(q, unique=True)
+        eoff, ekeys = oracle.match(f, ko, k, q, unique=True)
+        assert np.array_equal(uoff, eoff) and np.array_equal(ukeys, ekeys)
+    tm.close()
+
+
+def test_small_workloads_against_reference_matcher():
+    g = np.load(golden("matcher_small.npz"))
+    for tag in ("a", "b"):
+        f, ko, k = workload.generate_filters(int(g[f"{tag}_n"]), int(g[f"{tag}_seed"]))
+        q = workload.generate_queries(int(g[f"{tag}_nq"]), f, int(g[f"{tag}_seed"]))
+        for max_p in (65536, 300, 17):
+            tm = engine_with(f, ko, k, max_p)
+            off, keys = tm.match_batch(q)
+            assert_same_multisets(off, keys, g[f"{tag}_off"], g[f"{tag}_keys"])
+            uoff, ukeys = tm.match_batch(q, unique=True)
+            assert np.array_equal(uoff, g[f"{tag}_uoff"]) and np.array_equal(ukeys, g[f"{tag}_ukeys"])
+            tm.close()
+
+
+def test_config0_against_reference_digest():
+    """1M filters x 10K queries, partitions <= 65,536: digests equal the reference test_matcher's."""
+    g = np.load(golden("config0_digest.npz"))
+    f, ko, k, q = workload.config("config0")
+    tm = engine_with(f, ko, k, 65536)
+    off, keys = tm.match_batch(q)
+    c, h = oracle.digest(off, keys)
+    assert np.array_equal(c, g["count"]) and np.array_equal(h, g["hash"])
+    uoff, ukeys = tm.match_batch(q, unique=True)
+    c, h = oracle.digest(uoff, ukeys)
+    assert np.array_equal(c, g["ucount"]) and np.array_equal(h, g["uhash"])
+    info = tm.table_info()
+    assert info["filters"] == f.shape[0] and info["partitions"] > 1
+    tm.close()
+
+
+@pytest.mark.parametrize("n,nq,seed,max_p", [(1, 5, 31, 1), (33, 50, 32, 1), (500, 200, 33, 7),
+                                              (5000, 700, 34, 64), (50000, 300, 35, 1000), (200000, 257, 36, 65536)])
+def test_random_differential(n, nq, seed, max_p):
+    f, ko, k = workload.generate_filters(n, seed)
+    q = workload.generate_queries(nq, f, seed)
+    check_against_oracle(f, ko, k, q, max_p)
+
+
+def test_partitioner_against_reference():
+    gold = load_partitions_golden()
+    for case in gold["fixtures"] + gold["random"]:
+        f = np.asarray(case["filters"], dtype=np.uint32) if "filters" in case else \
+            workload.generate_filters(case["n"], case["seed"])[0]
+        part, masks, sizes = balanced_partitioning(f, case["max_p"])
+        assert groups_from_assignment(part, len(sizes)) == groups_from_assignment(case["partition_of"],
+                                                                                   len(case["sizes"]))
+        assert sorted(tuple(int(x) for x in m) for m in masks) == sorted(tuple(m) for m in case["masks"])
+        assert sorted(sizes.tolist()) == sorted(case["sizes"])
+
+
+def test_partitioning_known_answers_on_gpu():
+    fx = read_fixtures()
+    PF = np.stack([filter_from_string(s) for s in fx["PF"]])
+    PQ = np.stack([filter_from_string(s) for s in fx["PQ"]])
+    part, masks, sizes = balanced_partitioning(PQ[:3], 5)
+    assert len(sizes) == 1 and set(part.tolist()) == {0}
+    part, masks, sizes = balanced_partitioning(PF[:3], 5)
+    assert sorted(tuple(m) for m in masks.tolist()) == sorted([tuple(PF[0].tolist()), tuple((PF[1] & PF[2]).tolist())])
+    part, masks, sizes = balanced_partitioning(PF, 3)
+    assert len(sizes) == 5
+    ml = [tuple(m) for m in masks.tolist()]
+    for want, members in [(PF[3], [3]), (PF[4] & PF[9], [4, 9]), (PF[1] & PF[2] & PF[8], [1, 2, 8])]:
+        pid = ml.index(tuple(want.tolist()))
+        assert all(part[i] == pid for i in members)
+    allf = np.concatenate([PF, PQ])
+    part, masks, sizes = balanced_partitioning(allf, 4)
+    for i in range(len(allf)):
+        assert oracle.subset_of(masks[part[i]], allf[i])
+
+
+def test_edge_cases():
+    ones = np.full(6, 0xFFFFFFFF, dtype=np.uint32)
+    zeros = np.zeros(6, dtype=np.uint32)
+    # empty table
+    tm = TagMatch()
+    tm.set_persistence(False)
+    tm.consolidate(1000, 1)
+    off, keys = tm.match_batch(np.stack([ones, zeros]))
+    assert off.tolist() == [0, 0, 0] and keys.size == 0
+    # empty batch
+    off, keys = tm.match_batch(np.zeros((0, 6), np.uint32))
+    assert off.tolist() == [0]
+    tm.close()
+    # corner bits, all-ones / all-zero queries, large and extreme keys (sort path)
+    fl = [filter_from_bits([0]), filter_from_bits([191]), filter_from_bits([0, 191]), filter_from_bits(range(192)),
+          filter_from_bits([5, 64, 127, 128])]
+    kl = [[0xFFFFFFFF, 0], [1 << 20], [7, 7 + (1 << 31)], [3], [2, 2, 2]]
+    ko = np.cumsum([0] + [len(set(x)) for x in kl]).astype(np.uint32)
+    kk = np.concatenate([np.unique(np.array(x, dtype=np.uint32)) for x in kl]).astype(np.uint32)
+    f = np.stack(fl)
+    qs = np.stack([ones, zeros, filter_from_bits([0, 191]), filter_from_bits([5, 64, 127, 128, 0]),
+                   filter_from_bits(range(191))])
+    for max_p in (1, 2, 1000):
+        check_against_oracle(f, ko, kk, qs, max_p)
+    # the all-zero filter matches every query (the reference's partitioner
+    # does not terminate on it; here it is a partition with an empty mask)
+    f2 = np.concatenate([f, zeros[None]])
+    ko2 = np.append(ko, ko[-1] + 1).astype(np.uint32)
+    kk2 = np.append(kk, 99).astype(np.uint32)
+    check_against_oracle(f2, ko2, kk2, qs, 1000)
+    check_against_oracle(f2, ko2, kk2, qs, 2)
+
+
+def test_single_bit_and_nested_filters():
+    """single_bit_filters / deepest_trie (test_tagmatch.cc:591-640) at several partition sizes."""
+    ones = np.full((1, 6), 0xFFFFFFFF, dtype=np.uint32)
+    single = np.stack([filter_from_bits([i]) for i in range(192)])
+    nested = np.stack([filter_from_bits(range(i + 1)) for i in range(192)])
+    ko = np.arange(193, dtype=np.uint32)
+    kk = np.arange(192, dtype=np.uint32)
+    for f in (single, nested):
+        for max_p in (1, 3, 1000):
+            tm = engine_with(f, ko, kk, max_p)
+            off, keys = tm.match_batch(ones, unique=True)
+            assert keys.tolist() == list(range(192))
+            tm.close()
+
+
+def test_many_queries_one_partition_chunks():
+    """More than 256 queries routed to one partition (several chunks), and
+    batches larger than the device batch limit."""
+    f, ko, k = workload.generate_filters(3000, 41)
+    q = workload.generate_queries(5000, f, 41, superset_fraction=0.9)
+    tm = engine_with(f, ko, k, 65536)
+    tm.set_batch_limit(1500)
+    off, keys = tm.match_batch(q)
+    ooff, okeys = oracle.match(f, ko, k, q)
+    assert_same_multisets(off, keys, ooff, okeys)
+    tm.close()
+
+
+def test_capacity_error_reports_required_size():
+    f, ko, k = workload.generate_filters(2000, 42)
+    q = workload.generate_queries(100, f, 42)
+    tm = engine_with(f, ko, k)
+    off, keys = tm.match_batch(q)
+    import ctypes
+    lib = _native.load()
+    out_off = np.zeros(101, dtype=np.uint64)
+    small = np.zeros(1, dtype=np.uint32)
+    nk = ctypes.c_uint64(0)
+    st = lib.tm_match_batch(tm._h, q.ctypes.data_as(_native.u32p), 100, 0, out_off.ctypes.data_as(_native.u64p),
+                            small.ctypes.data_as(_native.u32p), 1, ctypes.byref(nk))
+    assert st == _native.TM_ERR_CAPACITY and nk.value == keys.size
+    assert np.array_equal(out_off, off)
+    tm.close()
+
+
+def test_incremental_updates_and_database(tmp_path):
+    """add / remove / re-consolidate through the database file (tagmatch.cc:92-142)."""
+    a, b, c = filter_from_bits([1, 2]), filter_from_bits([3]), filter_from_bits([1, 2, 3])
+    tm = TagMatch()
+    tm.set_database_filename(str(tmp_path / "tm.db"))
+    tm.add(a, [10, 11])
+    tm.add(b, 20)
+    tm.consolidate(1000, 1)
+    q = np.stack([c])
+    assert tm.match_batch(q, unique=True)[1].tolist() == [10, 11, 20]
+    tm.remove(a, 10)
+    tm.add(c, 30)
+    tm.consolidate()
+    assert tm.match_batch(q, unique=True)[1].tolist() == [11, 20, 30]
+    tm.remove(b, 20)  # last key of b: b leaves the table
+    tm.consolidate()
+    assert tm.match_batch(q, unique=True)[1].tolist() == [11, 30]
+    assert tm.table_info()["filters"] == 2
+    # database file: partition_fib_entry records (u32 partition, 24-byte filter, u32 n, keys)
+    raw = (tmp_path / "tm.db").read_bytes()
+    assert len(raw) == (4 + 24 + 4 + 4) + (4 + 24 + 4 + 4)
+    tm.clear()
+    tm.consolidate()
+    assert tm.match_batch(q, unique=True)[1].tolist() == []
+    tm.close()
+
+
+def test_async_matches_batch():
+    """tm_match_async (match_handler semantics): every callback fires once,
+    queries issued before start() complete after it, stop() drains."""
+    f, ko, k = workload.generate_filters(20000, 43)
+    q = workload.generate_queries(600, f, 43)
+    tm = engine_with(f, ko, k, 4096)
+    off, keys = tm.match_batch(q)
+    uoff, ukeys = tm.match_batch(q, unique=True)
+    got = {}
+    lock = threading.Lock()
+
+    def handler(i):
+        def h(arr):
+            with lock:
+                assert i not in got
+                got[i] = arr
+        return h
+
+    tm.set_latency_limit_ms(5)
+    for i in range(300):
+        tm.match(q[i], handler(i), unique=(i % 2 == 1))
+    tm.start(4, 1)
+    for i in range(300, 600):
+        tm.match(q[i], handler(i), unique=(i % 2 == 1))
+    tm.stop()
+    assert len(got) == 600
+    for i in range(600):
+        if i % 2:
+            assert np.array_equal(got[i], ukeys[uoff[i]:uoff[i + 1]])
+        else:
+            assert np.array_equal(np.sort(got[i]), np.sort(keys[off[i]:off[i + 1]]))
+    tm.close()
+
+
+def test_facade_cpp_cases(tmp_path):
+    """test/test_tagmatch.cc's cases through the tagmatch.hh-compatible C++ API."""
+    out = subprocess.run([build.FACADE_TEST, golden("tagmatch_fixtures.txt"), str(tmp_path / "tagmatch.db")],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "0 failures" in out.stdout
+
+
+def test_config1_table_sampled_parity():
+    """10M-filter table (seed 2): sampled queries against the oracle, and
+    size-independent properties of the full result (unique is the sorted
+    de-duplicated match set)."""
+    f, ko, k, q = workload.config("config1", n_queries=20000)
+    tm = engine_with(f, ko, k, 65536)
+    off, keys = tm.match_batch(q)
+    uoff, ukeys = tm.match_batch(q, unique=True)
+    sample = np.arange(0, 20000, 400)
+    so, sk = oracle.match(f, ko, k, q[sample])
+    for j, i in enumerate(sample):
+        assert np.array_equal(np.sort(keys[off[i]:off[i + 1]]), np.sort(sk[so[j]:so[j + 1]]))
+    for i in range(0, 20000, 97):
+        assert np.array_equal(np.unique(keys[off[i]:off[i + 1]]), ukeys[uoff[i]:uoff[i + 1]])
+    tm.close()
