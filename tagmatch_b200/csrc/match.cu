@@ -15,16 +15,24 @@
 //                shared memory); CTA-local counts reserve queue space with
 //                one global atomic per (CTA, partition); queue records are
 //                32 bytes (6 query words, query id, pad);
-//   k_plan       work items = (partition, 256-query chunk, 128-tile segment);
-//   k_match      persistent CTAs take items from an atomic counter, stage the
-//                chunk's queries into shared memory with one bulk TMA copy
-//                (cp.async.bulk + mbarrier), and give each warp one tile of
-//                <= 32 filters in registers: a lane-parallel test of the
-//                tile's AND mask against the chunk selects candidate queries
-//                (ballot), each candidate is tested against the 32 filters
-//                with 6 LOP3s, hits are compacted with ballot/popc into a
+//   host plan    work items = (partition, 256-query chunk, 128-tile segment),
+//                offsets computed on the host from the per-partition counts;
+//   k_slices     per 256-query chunk, bit-sliced "lacks bit b" masks:
+//                Z[b] bit j set when query j of the chunk lacks bit b
+//                (192 x 256 bits, ballot per bit);
+//   k_match      persistent CTAs take items from an atomic counter.  Each
+//                item's queries and slices are staged into shared memory by
+//                bulk TMA copies (cp.async.bulk + mbarrier), double-buffered:
+//                the next item loads while this one is matched, and the
+//                buffer is released by per-warp mbarrier arrivals instead of
+//                a CTA barrier.  Each warp takes one tile of <= 32 filters in
+//                registers; the tile's AND mask selects candidate queries by
+//                OR-ing the slices of its bits (8 lanes, one 32-query word
+//                each); each candidate is tested against the 32 filters with
+//                6 LOP3s; hits are compacted with ballot/popc into a
 //                per-warp shared-memory buffer flushed with one global atomic;
-//   k_key_count / k_key_fill   per-query key counts, prefix sums, key copy;
+//   k_key_count / k_key_fill   per-query key counts (warp-aggregated atomics
+//                over lanes holding the same query), prefix sums, key copy;
 //   k_unique_*   match_unique: per-query bitmap (small key spaces, output
 //                comes out sorted) or per-query block radix sort + unique.
 // Result overflow is exact: the pair buffer is regrown and the batch re-run
@@ -95,14 +103,42 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const uint32_t *__restr
     }
 }
 
-// Items per partition: query chunks x tile segments.
-__global__ void k_plan(const uint32_t *__restrict__ part_count, const uint32_t *__restrict__ part_tile_begin, uint32_t n_parts,
-                       uint32_t *__restrict__ item_count) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= n_parts) return;
-    const uint32_t nq = part_count[p];
-    const uint32_t nt = part_tile_begin[p + 1] - part_tile_begin[p];
-    item_count[p] = ((nq + kChunk - 1) / kChunk) * ((nt + kSegTiles - 1) / kSegTiles);
+// Bit-sliced query masks of one 256-query chunk: z[b * 8 + w] bit l is set
+// when query 32 w + l of the chunk lacks filter bit b, or does not exist
+// (so an absent query is never a candidate).
+__global__ void __launch_bounds__(kChunk) k_slices(const uint32_t *__restrict__ queue, const uint32_t *__restrict__ part_off,
+                                                   const uint32_t *__restrict__ part_count,
+                                                   const uint32_t *__restrict__ chunk_off, uint32_t n_parts,
+                                                   uint32_t *__restrict__ slices) {
+    const uint32_t c = blockIdx.x;
+    uint32_t lo = 0, hi = n_parts;  // partition of this chunk: chunk_off[lo] <= c < chunk_off[lo + 1]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (chunk_off[mid] <= c) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t p = lo;
+    const uint32_t chunk = c - chunk_off[p];
+    const uint32_t nq = min((uint32_t)kChunk, part_count[p] - chunk * kChunk);
+    const unsigned lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t j = w * 32 + lane;
+    uint32_t q[kWords];
+    const bool valid = j < nq;
+#pragma unroll
+    for (int k = 0; k < kWords; ++k)
+        q[k] = valid ? queue[size_t(part_off[p] + chunk * kChunk + j) * kQueueWords + k] : 0u;
+    uint32_t mine[kWords];
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) {
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+            const uint32_t z = __ballot_sync(kFull, !valid || !((q[k] >> b) & 1u));
+            if (lane == (unsigned)b) mine[k] = z;
+        }
+    }
+    uint32_t *zc = slices + size_t(c) * kBits * 8;
+#pragma unroll
+    for (int k = 0; k < kWords; ++k) zc[(k * 32 + lane) * 8 + w] = mine[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -144,11 +180,21 @@ struct MatchArgs {
     const uint32_t *part_count;
     const uint32_t *part_off;
     const uint32_t *item_off;
+    const uint32_t *chunk_off;
     const uint32_t *queue;
+    const uint32_t *slices;
     uint32_t n_parts;
     unsigned long long *counters;  // [0] next item, [1] pairs, [2] error flags
     Pair *pairs;
     unsigned long long pair_cap;
+};
+
+constexpr int kSliceWords = kBits * 8;  // 192 x 256 bits
+
+// One staging buffer: a chunk's query records and slices.
+struct __align__(128) Stage {
+    uint32_t q[kChunk * kQueueWords];  // 8 KB
+    uint32_t z[kSliceWords];           // 6 KB
 };
 
 __device__ __forceinline__ void flush_warp(Pair *buf, uint32_t n, const MatchArgs &a, unsigned lane) {
@@ -161,114 +207,161 @@ __device__ __forceinline__ void flush_warp(Pair *buf, uint32_t n, const MatchArg
     __syncwarp();
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false when the limit expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    unsigned long long spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++spins > kSpinLimit) return false;
+    }
+    return true;
+}
+
+struct ItemRef {
+    uint32_t p, qbase, nq, tb, te, zchunk;
+};
+
+__device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
+    uint32_t lo = 0, hi = a.n_parts;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.item_off[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    ItemRef r;
+    r.p = lo;
+    const uint32_t local = item - a.item_off[lo];
+    const uint32_t pq = a.part_count[lo];
+    const uint32_t nchunks = (pq + kChunk - 1) / kChunk;
+    const uint32_t chunk = local % nchunks, seg = local / nchunks;
+    r.qbase = a.part_off[lo] + chunk * kChunk;
+    r.nq = min((uint32_t)kChunk, pq - chunk * kChunk);
+    r.tb = a.part_tile_begin[lo] + seg * kSegTiles;
+    r.te = min(r.tb + (uint32_t)kSegTiles, a.part_tile_begin[lo + 1]);
+    r.zchunk = a.chunk_off[lo] + chunk;
+    return r;
+}
+
+// Thread 0: claim the next item and start its copy into stage `buf`; the
+// item id is published through the full barrier's phase completion.
+__device__ __forceinline__ void produce(const MatchArgs &a, uint32_t total, Stage *st, uint64_t *full, uint32_t *s_item,
+                                        int buf) {
+    const uint32_t item = uint32_t(atomicAdd(&a.counters[0], 1ull));
+    s_item[buf] = item;
+    if (item < total) {
+        const ItemRef r = locate(a, item);
+        const uint32_t qbytes = r.nq * kQueueWords * sizeof(uint32_t);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&full[buf], qbytes + kSliceWords * sizeof(uint32_t));
+        tma_bulk_g2s(st[buf].q, a.queue + size_t(r.qbase) * kQueueWords, qbytes, &full[buf]);
+        tma_bulk_g2s(st[buf].z, a.slices + size_t(r.zchunk) * kSliceWords, kSliceWords * sizeof(uint32_t), &full[buf]);
+    } else {
+        mbar_arrive(&full[buf]);  // nothing to copy: complete the phase so consumers see the end
+    }
+}
+
 __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
-    __shared__ __align__(128) uint32_t s_q[kChunk * kQueueWords];   // staged queries, 32 B each
+    __shared__ Stage st[2];
     __shared__ __align__(16) Pair s_out[kMatchWarps][kWarpBuf];
-    __shared__ __align__(8) uint64_t s_bar;
-    __shared__ uint32_t s_item, s_fail;
+    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ uint32_t s_item[2];
+    __shared__ int s_fail;
     const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t total = a.item_off[a.n_parts];
     if (tid == 0) {
-        mbar_init(&s_bar, 1);
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(&empty[0], kMatchWarps);
+        mbar_init(&empty[1], kMatchWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
     __syncthreads();
-    const uint32_t total = a.item_off[a.n_parts];
-    uint32_t phase = 0;
+    if (tid == 0) produce(a, total, st, full, s_item, 0);
     uint32_t nout = 0;  // staged pairs in this warp's buffer
-    for (;;) {
-        if (tid == 0) s_item = uint32_t(atomicAdd(&a.counters[0], 1ull));
-        __syncthreads();
-        const uint32_t item = s_item;
-        if (item >= total || s_fail) break;
-        // locate (partition, segment, chunk)
-        uint32_t lo = 0, hi = a.n_parts;
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (a.item_off[mid] <= item) lo = mid;
-            else hi = mid;
-        }
-        const uint32_t p = lo;
-        const uint32_t local = item - a.item_off[p];
-        const uint32_t pq = a.part_count[p];
-        const uint32_t nchunks = (pq + kChunk - 1) / kChunk;
-        const uint32_t chunk = local % nchunks, seg = local / nchunks;
-        const uint32_t qbase = a.part_off[p] + chunk * kChunk;
-        const uint32_t nq = min((uint32_t)kChunk, pq - chunk * kChunk);
-        const uint32_t tb = a.part_tile_begin[p] + seg * kSegTiles;
-        const uint32_t te = min(tb + (uint32_t)kSegTiles, a.part_tile_begin[p + 1]);
+    for (uint32_t it = 0;; ++it) {
+        const int b = it & 1;
+        // prefetch the next item into the other stage once every warp has
+        // released it (it held item it - 1)
         if (tid == 0) {
-            // order earlier generic reads of s_q before the async-proxy write
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            const uint32_t bytes = nq * kQueueWords * sizeof(uint32_t);
-            mbar_expect_tx(&s_bar, bytes);
-            tma_bulk_g2s(s_q, a.queue + size_t(qbase) * kQueueWords, bytes, &s_bar);
+            bool ok = true;
+            if (it >= 1) ok = mbar_wait(&empty[b ^ 1], ((it - 1) >> 1) & 1);
+            if (ok) produce(a, total, st, full, s_item, b ^ 1);
+            else { atomicOr(&a.counters[2], 1ull); s_fail = 1; }
         }
-        // bounded wait for the copy
-        {
-            unsigned long long spins = 0;
-            while (!mbar_try_wait(&s_bar, phase)) {
-                if (++spins > kSpinLimit) {
-                    atomicOr(&a.counters[2], 1ull);
-                    s_fail = 1;
-                    break;
-                }
-            }
+        if (!mbar_wait(&full[b], (it >> 1) & 1)) {
+            atomicOr(&a.counters[2], 2ull);
+            break;
         }
-        phase ^= 1;
-        __syncthreads();
-        if (s_fail) break;
-        const uint4 *sq = reinterpret_cast<const uint4 *>(s_q);
-        for (uint32_t t = tb + warp; t < te; t += kMatchWarps) {
+        const uint32_t item = s_item[b];
+        if (item >= total || s_fail) break;
+        const ItemRef r = locate(a, item);
+        const uint4 *sq = reinterpret_cast<const uint4 *>(st[b].q);
+        const uint32_t *sz = st[b].z;
+        for (uint32_t t = r.tb + warp; t < r.te; t += kMatchWarps) {
             uint32_t f[kWords];
 #pragma unroll
             for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
             const TileInfo ti = a.tile_info[t];
             const bool lane_valid = lane < ti.count;
-            // candidate selection on the tile's AND mask
-            for (uint32_t g = 0; g < nq; g += 32) {
-                const uint32_t j = g + lane;
-                bool pass = false;
-                if (j < nq) {
-                    const uint4 q0 = sq[j * 2], q1 = sq[j * 2 + 1];
-                    uint32_t acc = ti.and_mask[0] & ~q0.x;
-                    acc = andnot_or(ti.and_mask[1], q0.y, acc);
-                    acc = andnot_or(ti.and_mask[2], q0.z, acc);
-                    acc = andnot_or(ti.and_mask[3], q0.w, acc);
-                    acc = andnot_or(ti.and_mask[4], q1.x, acc);
-                    acc = andnot_or(ti.and_mask[5], q1.y, acc);
-                    pass = acc == 0;
+            // candidates: queries holding every bit of the tile's AND mask;
+            // lane w < 8 builds the word for queries 32 w .. 32 w + 31
+            uint32_t lack = 0;
+#pragma unroll
+            for (int k = 0; k < kWords; ++k) {
+                uint32_t m = ti.and_mask[k];
+                while (m) {
+                    const uint32_t bit = k * 32 + __ffs(m) - 1;
+                    m &= m - 1;
+                    if (lane < 8) lack |= sz[bit * 8 + lane];
                 }
-                uint32_t cand = __ballot_sync(kFull, pass);
-                while (cand) {
-                    const uint32_t jj = g + __ffs(cand) - 1;
-                    cand &= cand - 1;
-                    const uint4 q0 = sq[jj * 2], q1 = sq[jj * 2 + 1];
-                    uint32_t acc = f[0] & ~q0.x;
-                    acc = andnot_or(f[1], q0.y, acc);
-                    acc = andnot_or(f[2], q0.z, acc);
-                    acc = andnot_or(f[3], q0.w, acc);
-                    acc = andnot_or(f[4], q1.x, acc);
-                    acc = andnot_or(f[5], q1.y, acc);
-                    const bool hit = lane_valid && acc == 0;
-                    const uint32_t hm = __ballot_sync(kFull, hit);
-                    if (hm) {
-                        const uint32_t nh = __popc(hm);
-                        if (nout + nh > (uint32_t)kWarpBuf) {
+            }
+            uint32_t cand_word = lane < 8 ? ~lack : 0u;
+            if (lane < 8 && lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
+            for (uint32_t g = 0; g < 8; ++g) {
+                uint32_t c = __shfl_sync(kFull, cand_word, g);
+                while (c) {
+                    const uint32_t j0 = g * 32 + __ffs(c) - 1;
+                    c &= c - 1;
+                    const bool two = c != 0;
+                    const uint32_t j1 = two ? g * 32 + __ffs(c) - 1 : j0;
+                    c &= c - 1;
+                    const uint4 a0 = sq[j0 * 2], a1 = sq[j0 * 2 + 1];
+                    const uint4 b0 = sq[j1 * 2], b1 = sq[j1 * 2 + 1];
+                    uint32_t x = f[0] & ~a0.x, y = f[0] & ~b0.x;
+                    x = andnot_or(f[1], a0.y, x);
+                    y = andnot_or(f[1], b0.y, y);
+                    x = andnot_or(f[2], a0.z, x);
+                    y = andnot_or(f[2], b0.z, y);
+                    x = andnot_or(f[3], a0.w, x);
+                    y = andnot_or(f[3], b0.w, y);
+                    x = andnot_or(f[4], a1.x, x);
+                    y = andnot_or(f[4], b1.x, y);
+                    x = andnot_or(f[5], a1.y, x);
+                    y = andnot_or(f[5], b1.y, y);
+                    const bool h0 = lane_valid && x == 0;
+                    const bool h1 = two && lane_valid && y == 0;
+                    const uint32_t m0 = __ballot_sync(kFull, h0), m1 = __ballot_sync(kFull, h1);
+                    if (m0 | m1) {
+                        const uint32_t n0 = __popc(m0), n1 = __popc(m1);
+                        if (nout + n0 + n1 > (uint32_t)kWarpBuf) {
                             flush_warp(s_out[warp], nout, a, lane);
                             nout = 0;
                         }
-                        if (hit) {
-                            const uint32_t r = __popc(hm & ((1u << lane) - 1u));
-                            s_out[warp][nout + r] = Pair{q1.z, t * kTile + lane};
-                        }
-                        nout += nh;
+                        const uint32_t below = (1u << lane) - 1u;
+                        if (h0) s_out[warp][nout + __popc(m0 & below)] = Pair{a1.z, t * kTile + lane};
+                        if (h1) s_out[warp][nout + n0 + __popc(m1 & below)] = Pair{b1.z, t * kTile + lane};
+                        nout += n0 + n1;
                         __syncwarp();
                     }
                 }
             }
         }
-        __syncthreads();  // all reads of s_q done before the next copy
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[b]);
     }
     if (nout) flush_warp(s_out[warp], nout, a, lane);
 }
@@ -276,13 +369,41 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
 // ---------------------------------------------------------------------------
 // Key gather
 // ---------------------------------------------------------------------------
+// Lanes of a warp that hold pairs of the same query form one group
+// (__match_any_sync); each lane gets the sum of its group's key counts and
+// the part of it held by lower lanes, so a group needs one atomic.
+__device__ __forceinline__ void group_sums(uint32_t peers, uint32_t nk, unsigned lane, uint32_t &excl, uint32_t &tot) {
+    excl = 0;
+    tot = 0;
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+        const uint32_t v = __shfl_sync(kFull, nk, l);
+        if ((peers >> l) & 1u) {
+            tot += v;
+            if ((unsigned)l < lane) excl += v;
+        }
+    }
+}
+
 __global__ void k_key_count(const Pair *__restrict__ pairs, const unsigned long long *__restrict__ counters,
                             const uint32_t *__restrict__ slot_key_off, uint32_t *__restrict__ qkeys) {
     const unsigned long long n = counters[1];
-    for (unsigned long long i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
-        const Pair pr = pairs[i];
-        const uint32_t nk = slot_key_off[pr.slot + 1] - slot_key_off[pr.slot];
-        if (nk) atomicAdd(&qkeys[pr.query], nk);
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+    for (unsigned long long base = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x - lane); base < n;
+         base += warps * 32) {
+        const unsigned long long i = base + lane;
+        const bool valid = i < n;
+        Pair pr{0xFFFFFFFFu, 0u};
+        uint32_t nk = 0;
+        if (valid) {
+            pr = pairs[i];
+            nk = slot_key_off[pr.slot + 1] - slot_key_off[pr.slot];
+        }
+        const uint32_t peers = __match_any_sync(kFull, pr.query);
+        uint32_t excl, tot;
+        group_sums(peers, nk, lane, excl, tot);
+        if (valid && lane == (unsigned)(__ffs(peers) - 1) && tot) atomicAdd(&qkeys[pr.query], tot);
     }
 }
 
@@ -290,12 +411,27 @@ __global__ void k_key_fill(const Pair *__restrict__ pairs, const unsigned long l
                            const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
                            const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor, uint32_t *__restrict__ out) {
     const unsigned long long n = counters[1];
-    for (unsigned long long i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
-        const Pair pr = pairs[i];
-        const uint32_t b = slot_key_off[pr.slot], e = slot_key_off[pr.slot + 1];
-        if (e == b) continue;
-        uint64_t d = qoff[pr.query] + atomicAdd(&qcursor[pr.query], e - b);
-        for (uint32_t k = b; k < e; ++k) out[d++] = tkeys[k];
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+    for (unsigned long long base = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x - lane); base < n;
+         base += warps * 32) {
+        const unsigned long long i = base + lane;
+        const bool valid = i < n;
+        Pair pr{0xFFFFFFFFu, 0u};
+        uint32_t b = 0, e = 0;
+        if (valid) {
+            pr = pairs[i];
+            b = slot_key_off[pr.slot];
+            e = slot_key_off[pr.slot + 1];
+        }
+        const uint32_t peers = __match_any_sync(kFull, pr.query);
+        uint32_t excl, tot;
+        group_sums(peers, e - b, lane, excl, tot);
+        const unsigned leader = __ffs(peers) - 1;
+        uint64_t pos = 0;
+        if (valid && lane == leader && tot) pos = qoff[pr.query] + atomicAdd(&qcursor[pr.query], tot);
+        pos = __shfl_sync(kFull, pos, leader) + excl;
+        for (uint32_t k = b; k < e; ++k) out[pos++] = tkeys[k];
     }
 }
 
@@ -424,8 +560,9 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     part_off = std::move(o.part_off);
     part_cursor = std::move(o.part_cursor);
     queue = std::move(o.queue);
-    item_count = std::move(o.item_count);
     item_off = std::move(o.item_off);
+    chunk_off = std::move(o.chunk_off);
+    slices = std::move(o.slices);
     counters = std::move(o.counters);
     pairs = std::move(o.pairs);
     qkeys = std::move(o.qkeys);
@@ -499,7 +636,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     bs.routed = routed;
     for (uint32_t p = 0; p < P; ++p) bs.dense += uint64_t(s.h_part_count[p]) * t.h_part_size[p];
     const uint32_t windows = (P + kMaxRouteParts - 1) / kMaxRouteParts;
-    bs.launches += 2 * windows + 2 + 2 * scan_launches(P) + 1;  // route x2, plan, match, scans
+    bs.launches += 2 * windows + 2 + scan_launches(P);  // route x2, slices, match, scan
     s.queue.reserve(size_t(std::max<uint32_t>(routed, 1)) * kQueueWords + kChunk * kQueueWords);
     for (uint32_t p0 = 0; p0 < P; p0 += kMaxRouteParts) {
         const uint32_t pw = std::min(kMaxRouteParts, P - p0);
@@ -508,12 +645,30 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
                                                            s.part_cursor.p, s.queue.p);
         TM_CHECK_LAUNCH();
     }
-    // ---- plan ----
-    s.item_count.reserve(P);
+    // ---- plan: chunks and work items per partition (host, from the counts) ----
+    s.h_chunk_off.resize(size_t(P) + 1);
+    s.h_item_off.resize(size_t(P) + 1);
+    uint32_t chunks = 0, items = 0;
+    for (uint32_t p = 0; p < P; ++p) {
+        s.h_chunk_off[p] = chunks;
+        s.h_item_off[p] = items;
+        const uint32_t nc = (s.h_part_count[p] + kChunk - 1) / kChunk;
+        const uint32_t nt = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
+        chunks += nc;
+        items += nc * ((nt + kSegTiles - 1) / kSegTiles);
+    }
+    s.h_chunk_off[P] = chunks;
+    s.h_item_off[P] = items;
     s.item_off.reserve(size_t(P) + 1);
-    k_plan<<<blocks_for(P, 256), 256, 0, st>>>(s.part_count.p, t.part_tile_begin.p, P, s.item_count.p);
-    TM_CHECK_LAUNCH();
-    exclusive_scan<uint32_t, uint32_t>(s.item_count.p, s.item_off.p, P, s.scr, st);
+    s.chunk_off.reserve(size_t(P) + 1);
+    TM_CUDA(cudaMemcpyAsync(s.item_off.p, s.h_item_off.data(), (size_t(P) + 1) * 4, cudaMemcpyHostToDevice, st));
+    TM_CUDA(cudaMemcpyAsync(s.chunk_off.p, s.h_chunk_off.data(), (size_t(P) + 1) * 4, cudaMemcpyHostToDevice, st));
+    s.slices.reserve(size_t(std::max<uint32_t>(chunks, 1)) * kBits * 8);
+    if (chunks) {
+        k_slices<<<chunks, kChunk, 0, st>>>(s.queue.p, s.part_off.p, s.part_count.p, s.chunk_off.p, P, s.slices.p);
+        TM_CHECK_LAUNCH();
+    }
+    bs.items = items;
     // ---- match (regrow and re-run on pair overflow) ----
     if (s.pair_cap_hint == 0) s.pair_cap_hint = size_t(nq) * 1024 + (1u << 20);
     s.pairs.reserve(s.pair_cap_hint);
@@ -521,7 +676,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     for (int attempt = 0;; ++attempt) {
         TM_CUDA(cudaMemsetAsync(s.counters.p, 0, 4 * sizeof(unsigned long long), st));
         MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, s.part_count.p, s.part_off.p, s.item_off.p,
-                    s.queue.p, P, s.counters.p, s.pairs.p, (unsigned long long)s.pairs.cap};
+                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.counters.p, s.pairs.p, (unsigned long long)s.pairs.cap};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
             if (!s.ev_begin) {
@@ -535,10 +690,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         if (s.profile) TM_CUDA(cudaEventRecord(s.ev_end, st));
         if (match_end) TM_CUDA(cudaEventRecord(match_end, st));
         TM_CUDA(cudaMemcpyAsync(hc, s.counters.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-        uint32_t items = 0;
-        TM_CUDA(cudaMemcpyAsync(&items, s.item_off.p + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         TM_CUDA(cudaStreamSynchronize(st));
-        hc[3] = items;
         if (hc[2]) throw Error(TM_ERR_TIMEOUT, "match kernel: bounded wait for the query copy expired");
         if (s.profile) {
             float ms = 0.f;
@@ -551,7 +703,6 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         s.pairs.reserve(s.pair_cap_hint);
         bs.retries++;
     }
-    bs.items = hc[3];
     bs.pairs = hc[1];
     // ---- keys ----
     TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));

@@ -15,8 +15,9 @@ struct MatchScratch {
     DevBuf<uint32_t> part_off;    // [P + 1]
     DevBuf<uint32_t> part_cursor; // [P]
     DevBuf<uint32_t> queue;       // [routed][8]
-    DevBuf<uint32_t> item_count;  // [P]
-    DevBuf<uint32_t> item_off;    // [P + 1]
+    DevBuf<uint32_t> item_off;    // [P + 1] work items per partition (prefix)
+    DevBuf<uint32_t> chunk_off;   // [P + 1] 256-query chunks per partition (prefix)
+    DevBuf<uint32_t> slices;      // [chunks][192][8] bit-sliced "lacks bit" masks
     DevBuf<unsigned long long> counters;  // [0] work item, [1] pairs, [2] error flags
     DevBuf<Pair> pairs;
     DevBuf<uint32_t> qkeys;       // [nq]
@@ -26,7 +27,7 @@ struct MatchScratch {
     DevBuf<uint32_t> ucount;      // [nq]
     DevBuf<uint64_t> uoff;        // [nq + 1]
     DevBuf<uint32_t> ukeys;       // [total unique] (also radix temp)
-    std::vector<uint32_t> h_part_count;
+    std::vector<uint32_t> h_part_count, h_chunk_off, h_item_off;
     ScanScratch scr;
     int sm_count = 0;
     size_t pair_cap_hint = 0;

@@ -21,12 +21,15 @@
 //   k_children classifies the two sides into the next active list, the
 //              partition list, or (table builds) the tile list.
 //
-// For the matcher table each partition is then split the same way (balanced
-// pivot among bits not yet used inside that partition) down to tiles of at
-// most 32 filters; the AND of a tile's members lets the matcher skip the
-// whole tile for any query that lacks one of those bits.
+// For the matcher table each partition is then split further, down to tiles
+// of at most 32 filters.  The AND of a tile's members lets the matcher skip
+// the whole tile for any query that lacks one of those bits, so these splits
+// pick the bit (not yet used inside the partition) that maximises
+// (members holding it) x (estimated chance that a query lacks it), the
+// chance estimated from the bit's frequency over the whole table.
 #include "partition.cuh"
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 namespace tmb {
@@ -36,6 +39,11 @@ constexpr int kPChunk = 1024;  // filters per partitioner chunk
 constexpr int kPThreads = 256;
 constexpr uint32_t kActFinal = 0x100;
 constexpr uint32_t kActChop = 0x200;
+// Exponent of the tile-split weight (1 - table frequency of the bit)^k.  A
+// query is roughly the union of several stored tag sets, so a bit that is
+// frequent in the table is very likely present in a query; k ~ 10-16
+// minimised candidate (query, tile) pairs on the seeded workloads.
+constexpr double kTileWeightExp = 12.0;
 
 struct Counters {
     uint32_t next;
@@ -106,7 +114,7 @@ __device__ __forceinline__ unsigned long long warp_min_u64(unsigned long long v)
 }
 
 __global__ void k_decide(const Seg *__restrict__ segs, uint32_t n_act, const uint32_t *__restrict__ freq,
-                         uint32_t *__restrict__ action) {
+                         const float *__restrict__ tile_weight, uint32_t *__restrict__ action) {
     const uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (s >= n_act) return;
@@ -135,8 +143,14 @@ __global__ void k_decide(const Seg *__restrict__ segs, uint32_t n_act, const uin
         } else if (phase == kPhasePeel) {
             key = ((unsigned long long)(0xFFFFFFFFu - f) << 8) | b;  // first maximum
         } else {
+            // tile phase: the bit whose one side prunes the most queries,
+            // scored as (members holding it) x (weight: estimated chance
+            // that a query lacks it); highest score, earliest bit
             const bool used = (seg.used[k] >> lane) & 1u;
-            if (f > 0 && f < size && !used) key = ((unsigned long long)dist << 8) | b;
+            if (f > 0 && f < size && !used) {
+                const float score = float(f) * tile_weight[b];
+                key = ((unsigned long long)(~__float_as_uint(score)) << 8) | b;
+            }
         }
         best = key < best ? key : best;
     }
@@ -367,8 +381,10 @@ void gpu_partition(const uint32_t *d_filters, uint32_t n, uint32_t max_p, bool w
     DevBuf<uint64_t> zoff;
     DevBuf<Range> finals, leaves;
     DevBuf<Counters> cnt;
+    DevBuf<float> weights;
     ScanScratch scr;
     cnt.reserve(1);
+    weights.reserve(kBits);
     uint32_t finals_cap = n + 1024;
     uint32_t leaves_cap = with_tiles ? n + 1 : 1;
     finals.reserve(finals_cap);
@@ -401,7 +417,19 @@ void gpu_partition(const uint32_t *d_filters, uint32_t n, uint32_t max_p, bool w
         k_freq<<<total_chunks, kPThreads, 0, st>>>(segs[cur].p, chunk_off.p, n_act, out.words.p, freq.p);
         TM_CHECK_LAUNCH();
         action.reserve(n_act);
-        k_decide<<<blocks_for(size_t(n_act) * 32, 256), 256, 0, st>>>(segs[cur].p, n_act, freq.p, action.p);
+        if (levels == 1) {
+            // bit frequencies of the whole table -> tile-split weights:
+            // a query lacks bit b with estimated probability
+            // (1 - freq_b / n)^kTileWeightExp
+            std::vector<uint32_t> rf(kBits);
+            TM_CUDA(cudaMemcpyAsync(rf.data(), freq.p, kBits * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+            TM_CUDA(cudaStreamSynchronize(st));
+            std::vector<float> w(kBits);
+            for (int b = 0; b < kBits; ++b) w[b] = float(std::pow(1.0 - double(rf[b]) / double(n), kTileWeightExp));
+            weights.reserve(kBits);
+            TM_CUDA(cudaMemcpyAsync(weights.p, w.data(), kBits * sizeof(float), cudaMemcpyHostToDevice, st));
+        }
+        k_decide<<<blocks_for(size_t(n_act) * 32, 256), 256, 0, st>>>(segs[cur].p, n_act, freq.p, weights.p, action.p);
         TM_CHECK_LAUNCH();
         zc.reserve(total_chunks);
         zoff.reserve(size_t(total_chunks) + 1);
