@@ -114,6 +114,25 @@ int tm_match_batch(tm_engine *e, const uint32_t *queries, uint64_t n, int unique
 int tm_match_batch_device(tm_engine *e, const uint32_t *d_queries, uint32_t n, int unique, const uint64_t **d_offsets,
                           const uint32_t **d_keys, uint64_t *n_keys, void *stream);
 
+/* No counterpart in the reference.  tm_match_batch_device without any device
+ * allocation, for callers that cannot call cudaMalloc while matching (a
+ * pool allocator owns the device memory, a serving thread cannot afford the
+ * device synchronisation an allocation may cause, or the CUDA allocator may
+ * not be entered where they run).  Every scratch buffer comes from one
+ * static device array of 64 MiB that each GPU loading this library holds
+ * until exit.  d_queries, d_out_offsets (n + 1 entries) and d_out_keys
+ * (capacity keys) are device memory owned by the caller; results are as in
+ * tm_match_batch.  Limits: n <= 4096 queries, tables of <= 16384
+ * partitions, and the call's scratch within the array -- otherwise
+ * TM_ERR_INVALID or TM_ERR_CAPACITY with a message saying what to split.
+ * The array is shared by all calls and keeps the last call's contents:
+ * calls whose work overlaps on the GPU (other threads, unordered streams)
+ * race.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+int tm_match_batch_device_noalloc(tm_engine *e, const uint32_t *d_queries, uint32_t n, int unique,
+                                  uint64_t *d_out_offsets, uint32_t *d_out_keys, uint64_t capacity, uint64_t *n_keys,
+                                  void *stream);
+
 /* tagmatch::match / match_unique with a handler (tagmatch.cc:200-210,
  * front_end.cc:540-551): queues one query; cb(user, tag, keys, n) fires
  * once, on an engine thread, after the query's batch completes. */

@@ -69,6 +69,9 @@ SIGNATURES = {
     "tm_match_batch_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
                                              ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), u64p,
                                              ctypes.c_void_p]),
+    "tm_match_batch_device_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, u64p,
+                                                     ctypes.c_void_p]),
     "tm_match_async": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_int, ctypes.c_uint64, MATCH_CALLBACK,
                                       ctypes.c_void_p]),
     "tm_balanced_partitioning": (ctypes.c_int, [u32p, ctypes.c_uint64, ctypes.c_uint32, u32p, u32p, u32p,

@@ -131,6 +131,16 @@ int tm_match_batch_device(tm_engine *e, const uint32_t *d_queries, uint32_t n, i
     });
 }
 
+int tm_match_batch_device_noalloc(tm_engine *e, const uint32_t *d_queries, uint32_t n, int unique,
+                                  uint64_t *d_out_offsets, uint32_t *d_out_keys, uint64_t capacity, uint64_t *n_keys,
+                                  void *stream) {
+    if (!e || !d_out_offsets || !n_keys || (n && !d_queries) || (capacity && !d_out_keys)) return TM_ERR_INVALID;
+    return guard(e, [&] {
+        e->eng.match_device_noalloc(d_queries, n, unique != 0, d_out_offsets, d_out_keys, capacity, n_keys,
+                                    static_cast<cudaStream_t>(stream));
+    });
+}
+
 int tm_match_async(tm_engine *e, const uint32_t query[TM_FILTER_WORDS], int unique, uint64_t tag, tm_match_callback cb,
                    void *user) {
     if (!e || !query) return TM_ERR_INVALID;

@@ -358,6 +358,16 @@ void Engine::match_device(const uint32_t *d_queries, uint32_t nq, bool unique, c
     if (bs) *bs = local;
 }
 
+void Engine::match_device_noalloc(const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_offsets,
+                                  uint32_t *d_keys, uint64_t capacity, uint64_t *n_keys, cudaStream_t st) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (!already_consolidated_ || devs_.empty() || !devs_[0]->table_ready || dev_version_[0] != table_version_)
+        throw Error(TM_ERR_STATE, "no device table: call consolidate() first");
+    Device &d = *devs_[0];
+    TM_CUDA(cudaSetDevice(d.id));
+    match_batch_noalloc(d.table, d_queries, nq, unique, d_offsets, d_keys, capacity, n_keys, st ? st : d.stream);
+}
+
 void Engine::set_profiling(bool on) {
     std::lock_guard<std::mutex> lk(api_mtx_);
     profile_ = on;

@@ -110,6 +110,10 @@ public:
     void match_device(const uint32_t *d_queries, uint32_t nq, bool unique, const uint64_t **d_offsets,
                       const uint32_t **d_keys, uint64_t *n_keys, cudaStream_t st, BatchStats *bs, cudaEvent_t ev0,
                       cudaEvent_t ev1);
+    // same as match_device, with every scratch buffer taken from a static
+    // device array (no allocation); outputs are caller-owned device memory
+    void match_device_noalloc(const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_offsets, uint32_t *d_keys,
+                              uint64_t capacity, uint64_t *n_keys, cudaStream_t st);
     // asynchronous match: cb fires exactly once per request, on an engine
     // thread, after start() (requests made earlier wait for it)
     void submit(const AsyncRequest &r);

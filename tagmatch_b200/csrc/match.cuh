@@ -61,4 +61,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
                  const uint64_t **d_offsets, const uint32_t **d_keys, uint64_t *n_keys, BatchStats *stats,
                  cudaStream_t st, cudaEvent_t match_begin = nullptr, cudaEvent_t match_end = nullptr);
 
+// The same pipeline with all scratch in a static device array (noalloc.cu).
+void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_out_offsets,
+                         uint32_t *d_out_keys, uint64_t capacity, uint64_t *n_keys, cudaStream_t st);
+
 }  // namespace tmb
