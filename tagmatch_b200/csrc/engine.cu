@@ -30,10 +30,12 @@ Engine::~Engine() {
     } catch (...) {
     }
     for (auto &d : devs_) {
-        if (d && d->stream) {
-            cudaSetDevice(d->id);
-            cudaStreamDestroy(d->stream);
-        }
+        if (!d) continue;
+        cudaSetDevice(d->id);
+        if (d->stream) cudaStreamDestroy(d->stream);
+        if (d->stream2) cudaStreamDestroy(d->stream2);
+        for (cudaEvent_t ev : d->lane_done)
+            if (ev) cudaEventDestroy(ev);
     }
 }
 
@@ -248,6 +250,7 @@ void Engine::clear() {
         TM_CUDA(cudaSetDevice(d->id));
         d->table = DevTable();
         d->scratch = MatchScratch();
+        d->scratch2 = MatchScratch();
         d->table_ready = false;
     }
 }
@@ -373,6 +376,41 @@ void Engine::set_profiling(bool on) {
     profile_ = on;
 }
 
+namespace {
+
+bool is_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// memcpy split over a few threads (pinned staging -> pageable caller memory)
+void parallel_copy(void *dst, const void *src, size_t bytes) {
+    const size_t kMin = size_t(64) << 20;
+    const int nt = int(std::min<size_t>(8, std::max<size_t>(1, bytes / kMin)));
+    if (nt == 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (int t = 0; t < nt; ++t) {
+        const size_t b = size_t(t) * per, e = std::min(bytes, b + per);
+        if (b < e)
+            th.emplace_back([=] { std::memcpy(static_cast<char *>(dst) + b, static_cast<const char *>(src) + b, e - b); });
+    }
+    for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+// Batches alternate between two lanes (scratch + stream + pinned staging):
+// while one batch's results travel to the host, the next batch is matched.
+// Keys go straight into a pinned caller buffer; a pageable one is filled
+// from pinned staging by copy threads.
 void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
                         uint64_t capacity, uint64_t *n_keys) {
     std::lock_guard<std::mutex> lk(api_mtx_);
@@ -380,29 +418,84 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     Device &d = device(0);
     if (dev_version_[0] != table_version_) build_device_table(d);
     TM_CUDA(cudaSetDevice(d.id));
+    if (!d.stream2) TM_CUDA(cudaStreamCreateWithFlags(&d.stream2, cudaStreamNonBlocking));
+    for (int l = 0; l < 2; ++l)
+        if (!d.lane_done[l]) TM_CUDA(cudaEventCreateWithFlags(&d.lane_done[l], cudaEventDisableTiming));
+    MatchScratch *scr[2] = {&d.scratch, &d.scratch2};
+    cudaStream_t str[2] = {d.stream, d.stream2};
+    HostBuf<uint64_t> *hoff[2] = {&d.h_offsets, &d.h_offsets2};
+    HostBuf<uint32_t> *hkeys[2] = {&d.h_keys, &d.h_keys2};
+    const bool direct = out_keys != nullptr && is_pinned(out_keys);
+    struct Pending {
+        bool active = false;
+        uint64_t q0 = 0, base = 0, nk = 0;
+        uint32_t n = 0;
+        bool staged = false;
+        std::thread copier;
+    } pend[2];
     uint64_t total = 0;
     bool overflow = false;
     out_offsets[0] = 0;
-    for (uint64_t q0 = 0; q0 < nq; q0 += batch_limit_) {
-        const uint32_t n = uint32_t(std::min<uint64_t>(batch_limit_, nq - q0));
-        d.scratch.queries.reserve(size_t(n) * kWords);
-        TM_CUDA(cudaMemcpyAsync(d.scratch.queries.p, queries + q0 * kWords, size_t(n) * 24, cudaMemcpyHostToDevice, d.stream));
-        const uint64_t *doff;
-        const uint32_t *dkeys;
-        uint64_t nk = 0;
-        BatchStats bs;
-        d.scratch.profile = profile_;
-        match_batch(d.table, d.scratch.queries.p, n, unique, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
-        stats_.add(bs, n, profile_);
-        TM_CUDA(cudaMemcpyAsync(out_offsets + q0 + 1, doff + 1, size_t(n) * 8, cudaMemcpyDeviceToHost, d.stream));
-        if (!overflow && total + nk <= capacity) {
-            if (nk) TM_CUDA(cudaMemcpyAsync(out_keys + total, dkeys, nk * 4, cudaMemcpyDeviceToHost, d.stream));
-        } else {
-            overflow = true;
+    auto finish = [&](int l) {
+        Pending &p = pend[l];
+        if (!p.active) return;
+        if (p.copier.joinable()) p.copier.join();
+        TM_CUDA(cudaStreamSynchronize(str[l]));
+        const uint64_t *o = hoff[l]->p;
+        for (uint32_t i = 1; i <= p.n; ++i) out_offsets[p.q0 + i] = o[i] + p.base;
+        p.active = false;
+    };
+    try {
+        uint64_t it = 0;
+        for (uint64_t q0 = 0; q0 < nq; q0 += batch_limit_, ++it) {
+            const int l = int(it & 1);
+            finish(l);
+            const uint32_t n = uint32_t(std::min<uint64_t>(batch_limit_, nq - q0));
+            MatchScratch &sc = *scr[l];
+            sc.queries.reserve(size_t(n) * kWords);
+            TM_CUDA(cudaMemcpyAsync(sc.queries.p, queries + q0 * kWords, size_t(n) * 24, cudaMemcpyHostToDevice, str[l]));
+            const uint64_t *doff;
+            const uint32_t *dkeys;
+            uint64_t nk = 0;
+            BatchStats bs;
+            sc.profile = profile_;
+            match_batch(d.table, sc.queries.p, n, unique, sc, &doff, &dkeys, &nk, &bs, str[l]);
+            stats_.add(bs, n, profile_);
+            hoff[l]->reserve(size_t(n) + 1);
+            TM_CUDA(cudaMemcpyAsync(hoff[l]->p, doff, (size_t(n) + 1) * 8, cudaMemcpyDeviceToHost, str[l]));
+            Pending &p = pend[l];
+            p.active = true;
+            p.q0 = q0;
+            p.n = n;
+            p.base = total;
+            p.nk = nk;
+            p.staged = false;
+            if (!overflow && total + nk <= capacity) {
+                if (nk && direct) {
+                    TM_CUDA(cudaMemcpyAsync(out_keys + total, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
+                } else if (nk) {
+                    hkeys[l]->reserve(nk);
+                    TM_CUDA(cudaMemcpyAsync(hkeys[l]->p, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
+                    TM_CUDA(cudaEventRecord(d.lane_done[l], str[l]));
+                    p.staged = true;
+                    cudaEvent_t ev = d.lane_done[l];
+                    uint32_t *dst = out_keys + total;
+                    const uint32_t *src = hkeys[l]->p;
+                    p.copier = std::thread([=] {
+                        if (cudaEventSynchronize(ev) == cudaSuccess) parallel_copy(dst, src, nk * 4);
+                    });
+                }
+            } else {
+                overflow = true;
+            }
+            total += nk;
         }
-        TM_CUDA(cudaStreamSynchronize(d.stream));
-        for (uint32_t i = 1; i <= n; ++i) out_offsets[q0 + i] += total;
-        total += nk;
+        finish(0);
+        finish(1);
+    } catch (...) {
+        for (int l = 0; l < 2; ++l)
+            if (pend[l].copier.joinable()) pend[l].copier.join();
+        throw;
     }
     *n_keys = total;
     if (overflow) throw Error(TM_ERR_CAPACITY, "output key buffer too small: " + std::to_string(total) + " keys needed");

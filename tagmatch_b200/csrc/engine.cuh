@@ -137,13 +137,14 @@ public:
 private:
     struct Device {
         int id = 0;
-        cudaStream_t stream = nullptr;
+        cudaStream_t stream = nullptr, stream2 = nullptr;
+        cudaEvent_t lane_done[2] = {nullptr, nullptr};
         DevTable table;
-        MatchScratch scratch;
+        MatchScratch scratch, scratch2;  // two pipeline lanes of match_host
         bool table_ready = false;
         HostBuf<uint32_t> h_queries;
-        HostBuf<uint64_t> h_offsets;
-        HostBuf<uint32_t> h_keys;
+        HostBuf<uint64_t> h_offsets, h_offsets2;
+        HostBuf<uint32_t> h_keys, h_keys2;
         std::thread worker;
     };
     void build_device_table(Device &d);

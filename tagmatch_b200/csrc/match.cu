@@ -38,6 +38,8 @@
 // Result overflow is exact: the pair buffer is regrown and the batch re-run
 // (the reference truncates silently at 4,194,304 hits, gpu.cu:55).
 #include "match_kernels.cuh"
+#include <cstdio>
+#include <cstdlib>
 
 namespace tmb {
 
@@ -51,6 +53,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     item_off = std::move(o.item_off);
     chunk_off = std::move(o.chunk_off);
     slices = std::move(o.slices);
+    work = std::move(o.work);
     counters = std::move(o.counters);
     pairs = std::move(o.pairs);
     qkeys = std::move(o.qkeys);
@@ -163,8 +166,14 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     unsigned long long hc[4] = {0, 0, 0, 0};
     for (int attempt = 0;; ++attempt) {
         TM_CUDA(cudaMemsetAsync(s.counters.p, 0, 4 * sizeof(unsigned long long), st));
+        static const bool work_counters = std::getenv("TM_WORK_COUNTERS") != nullptr;
+        if (work_counters) {
+            s.work.reserve(8);
+            TM_CUDA(cudaMemsetAsync(s.work.p, 0, 8 * sizeof(unsigned long long), st));
+        }
         MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, s.part_count.p, s.part_off.p, s.item_off.p,
-                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.counters.p, s.pairs.p, (unsigned long long)s.pairs.cap};
+                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.counters.p, s.pairs.p, (unsigned long long)s.pairs.cap,
+                    work_counters ? s.work.p : nullptr};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
             if (!s.ev_begin) {
@@ -173,13 +182,20 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             }
             TM_CUDA(cudaEventRecord(s.ev_begin, st));
         }
-        k_match<<<unsigned(s.sm_count) * 4, kMatchThreads, 0, st>>>(a);
+        if (work_counters) k_match<true><<<unsigned(s.sm_count) * 4, kMatchThreads, 0, st>>>(a);
+        else k_match<false><<<unsigned(s.sm_count) * 4, kMatchThreads, 0, st>>>(a);
         TM_CHECK_LAUNCH();
         if (s.profile) TM_CUDA(cudaEventRecord(s.ev_end, st));
         if (match_end) TM_CUDA(cudaEventRecord(match_end, st));
         TM_CUDA(cudaMemcpyAsync(hc, s.counters.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         TM_CUDA(cudaStreamSynchronize(st));
         if (hc[2]) throw Error(TM_ERR_TIMEOUT, "match kernel: bounded wait for the query copy expired");
+        if (work_counters) {
+            unsigned long long w[8];
+            TM_CUDA(cudaMemcpy(w, s.work.p, sizeof(w), cudaMemcpyDeviceToHost));
+            std::fprintf(stderr, "[tm work] queries %u tile_visits %llu and_bits %llu candidates %llu trips %llu items %llu pairs %llu\n",
+                         nq, w[0], w[1], w[2], w[3], w[4], hc[1]);
+        }
         if (s.profile) {
             float ms = 0.f;
             TM_CUDA(cudaEventElapsedTime(&ms, s.ev_begin, s.ev_end));

@@ -18,6 +18,7 @@ struct MatchScratch {
     DevBuf<uint32_t> item_off;    // [P + 1] work items per partition (prefix)
     DevBuf<uint32_t> chunk_off;   // [P + 1] 256-query chunks per partition (prefix)
     DevBuf<uint32_t> slices;      // [chunks][192][8] bit-sliced "lacks bit" masks
+    DevBuf<unsigned long long> work;  // optional kernel work counters
     DevBuf<unsigned long long> counters;  // [0] work item, [1] pairs, [2] error flags
     DevBuf<Pair> pairs;
     DevBuf<uint32_t> qkeys;       // [nq]

@@ -12,7 +12,7 @@ namespace {
 constexpr int kRouteThreads = 256;
 constexpr int kMatchThreads = 256;
 constexpr int kMatchWarps = kMatchThreads / 32;
-constexpr int kWarpBuf = 256;  // staged pairs per warp
+constexpr int kWarpBuf = 128;  // staged pairs per warp
 constexpr uint32_t kMaxRouteParts = 1536;  // partition masks per routing window (48 KB of shared memory)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
@@ -153,6 +153,10 @@ struct MatchArgs {
     unsigned long long *counters;  // [0] next item, [1] pairs, [2] error flags
     Pair *pairs;
     unsigned long long pair_cap;
+    // optional work counters (diagnostics): [0] tile visits, [1] AND-mask
+    // bits OR-ed, [2] candidate (query, tile) pairs, [3] candidate loop
+    // trips, [4] items; null when off
+    unsigned long long *work;
 };
 
 constexpr int kSliceWords = kBits * 8;  // 192 x 256 bits
@@ -229,9 +233,12 @@ __device__ __forceinline__ void produce(const MatchArgs &a, uint32_t total, Stag
     }
 }
 
+// COUNT: diagnostics instantiation that also tallies its work (a.work).
+template <bool COUNT>
 __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
     __shared__ Stage st[2];
     __shared__ __align__(16) Pair s_out[kMatchWarps][kWarpBuf];
+    __shared__ __align__(16) uint32_t s_list[kMatchWarps][kChunk + 4];  // per-warp candidate lists
     __shared__ __align__(8) uint64_t full[2], empty[2];
     __shared__ uint32_t s_item[2];
     __shared__ int s_fail;
@@ -248,6 +255,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
     __syncthreads();
     if (tid == 0) produce(a, total, st, full, s_item, 0);
     uint32_t nout = 0;  // staged pairs in this warp's buffer
+    uint32_t w_tiles = 0, w_bits = 0, w_cand = 0, w_trips = 0, w_items = 0;
     for (uint32_t it = 0;; ++it) {
         const int b = it & 1;
         // prefetch the next item into the other stage once every warp has
@@ -265,6 +273,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
         const uint32_t item = s_item[b];
         if (item >= total || s_fail) break;
         const ItemRef r = locate(a, item);
+        if (COUNT) ++w_items;
         const uint4 *sq = reinterpret_cast<const uint4 *>(st[b].q);
         const uint32_t *sz = st[b].z;
         for (uint32_t t = r.tb + warp; t < r.te; t += kMatchWarps) {
@@ -273,6 +282,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
             for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
             const TileInfo ti = a.tile_info[t];
             const bool lane_valid = lane < ti.count;
+            if (COUNT) ++w_tiles;
             // candidates: queries holding every bit of the tile's AND mask;
             // lane w < 8 builds the word for queries 32 w .. 32 w + 31
             uint32_t lack = 0;
@@ -282,54 +292,102 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
                 while (m) {
                     const uint32_t bit = k * 32 + __ffs(m) - 1;
                     m &= m - 1;
+                    if (COUNT) ++w_bits;
                     if (lane < 8) lack |= sz[bit * 8 + lane];
                 }
             }
             uint32_t cand_word = lane < 8 ? ~lack : 0u;
             if (lane < 8 && lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
-            for (uint32_t g = 0; g < 8; ++g) {
-                uint32_t c = __shfl_sync(kFull, cand_word, g);
+            // compact candidate list (uint4 index of each query record):
+            // lanes 0-7 write the queries of their 32-query word in order
+            const uint32_t cnt = __popc(cand_word);
+            uint32_t incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const uint32_t v = __shfl_up_sync(kFull, incl, o);
+                if (lane >= (unsigned)o) incl += v;
+            }
+            const uint32_t n = __shfl_sync(kFull, incl, 7);
+            if (COUNT) w_cand += cnt;
+            if (n == 0) continue;
+            uint32_t *list = s_list[warp];
+            if (lane < 8) {
+                uint32_t pos = incl - cnt, c = cand_word;
                 while (c) {
-                    const uint32_t j0 = g * 32 + __ffs(c) - 1;
+                    list[pos++] = (lane * 32 + __ffs(c) - 1) * 2;
                     c &= c - 1;
-                    const bool two = c != 0;
-                    const uint32_t j1 = two ? g * 32 + __ffs(c) - 1 : j0;
-                    c &= c - 1;
-                    const uint4 a0 = sq[j0 * 2], a1 = sq[j0 * 2 + 1];
-                    const uint4 b0 = sq[j1 * 2], b1 = sq[j1 * 2 + 1];
-                    uint32_t x = f[0] & ~a0.x, y = f[0] & ~b0.x;
-                    x = andnot_or(f[1], a0.y, x);
-                    y = andnot_or(f[1], b0.y, y);
-                    x = andnot_or(f[2], a0.z, x);
-                    y = andnot_or(f[2], b0.z, y);
-                    x = andnot_or(f[3], a0.w, x);
-                    y = andnot_or(f[3], b0.w, y);
-                    x = andnot_or(f[4], a1.x, x);
-                    y = andnot_or(f[4], b1.x, y);
-                    x = andnot_or(f[5], a1.y, x);
-                    y = andnot_or(f[5], b1.y, y);
-                    const bool h0 = lane_valid && x == 0;
-                    const bool h1 = two && lane_valid && y == 0;
+                }
+            } else if (lane < 12) {
+                list[n + lane - 8] = 0;  // pad to a multiple of 4 with a valid index
+            }
+            __syncwarp();
+            for (uint32_t i = 0; i < n; i += 4) {
+                if (COUNT) ++w_trips;
+                const uint4 idx = *reinterpret_cast<const uint4 *>(&list[i]);
+                const uint4 p0 = sq[idx.x], p1 = sq[idx.x + 1];
+                const uint4 q0 = sq[idx.y], q1 = sq[idx.y + 1];
+                const uint4 r0 = sq[idx.z], r1 = sq[idx.z + 1];
+                const uint4 u0 = sq[idx.w], u1 = sq[idx.w + 1];
+                uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
+                x0 = andnot_or(f[1], p0.y, x0);
+                x1 = andnot_or(f[1], q0.y, x1);
+                x2 = andnot_or(f[1], r0.y, x2);
+                x3 = andnot_or(f[1], u0.y, x3);
+                x0 = andnot_or(f[2], p0.z, x0);
+                x1 = andnot_or(f[2], q0.z, x1);
+                x2 = andnot_or(f[2], r0.z, x2);
+                x3 = andnot_or(f[2], u0.z, x3);
+                x0 = andnot_or(f[3], p0.w, x0);
+                x1 = andnot_or(f[3], q0.w, x1);
+                x2 = andnot_or(f[3], r0.w, x2);
+                x3 = andnot_or(f[3], u0.w, x3);
+                x0 = andnot_or(f[4], p1.x, x0);
+                x1 = andnot_or(f[4], q1.x, x1);
+                x2 = andnot_or(f[4], r1.x, x2);
+                x3 = andnot_or(f[4], u1.x, x3);
+                x0 = andnot_or(f[5], p1.y, x0);
+                x1 = andnot_or(f[5], q1.y, x1);
+                x2 = andnot_or(f[5], r1.y, x2);
+                x3 = andnot_or(f[5], u1.y, x3);
+                const bool h0 = lane_valid && x0 == 0;
+                const bool h1 = lane_valid && x1 == 0 && i + 1 < n;
+                const bool h2 = lane_valid && x2 == 0 && i + 2 < n;
+                const bool h3 = lane_valid && x3 == 0 && i + 3 < n;
+                if (__any_sync(kFull, h0 | h1 | h2 | h3)) {
                     const uint32_t m0 = __ballot_sync(kFull, h0), m1 = __ballot_sync(kFull, h1);
-                    if (m0 | m1) {
-                        const uint32_t n0 = __popc(m0), n1 = __popc(m1);
-                        if (nout + n0 + n1 > (uint32_t)kWarpBuf) {
-                            flush_warp(s_out[warp], nout, a, lane);
-                            nout = 0;
-                        }
-                        const uint32_t below = (1u << lane) - 1u;
-                        if (h0) s_out[warp][nout + __popc(m0 & below)] = Pair{a1.z, t * kTile + lane};
-                        if (h1) s_out[warp][nout + n0 + __popc(m1 & below)] = Pair{b1.z, t * kTile + lane};
-                        nout += n0 + n1;
-                        __syncwarp();
+                    const uint32_t m2 = __ballot_sync(kFull, h2), m3 = __ballot_sync(kFull, h3);
+                    const uint32_t nh = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+                    if (nout + nh > (uint32_t)kWarpBuf) {
+                        flush_warp(s_out[warp], nout, a, lane);
+                        nout = 0;
                     }
+                    const uint32_t below = (1u << lane) - 1u;
+                    const uint32_t slot = t * kTile + lane;
+                    uint32_t base = nout;
+                    if (h0) s_out[warp][base + __popc(m0 & below)] = Pair{p1.z, slot};
+                    base += __popc(m0);
+                    if (h1) s_out[warp][base + __popc(m1 & below)] = Pair{q1.z, slot};
+                    base += __popc(m1);
+                    if (h2) s_out[warp][base + __popc(m2 & below)] = Pair{r1.z, slot};
+                    base += __popc(m2);
+                    if (h3) s_out[warp][base + __popc(m3 & below)] = Pair{u1.z, slot};
+                    nout += nh;
+                    __syncwarp();
                 }
             }
+            __syncwarp();  // the list is rebuilt for the next tile
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[b]);
     }
     if (nout) flush_warp(s_out[warp], nout, a, lane);
+    if (COUNT && lane == 0) {
+        atomicAdd(&a.work[0], (unsigned long long)w_tiles);
+        atomicAdd(&a.work[1], (unsigned long long)w_bits);
+        atomicAdd(&a.work[2], (unsigned long long)w_cand);
+        atomicAdd(&a.work[3], (unsigned long long)w_trips);
+        if (warp == 0) atomicAdd(&a.work[4], (unsigned long long)w_items);
+    }
 }
 
 // ---------------------------------------------------------------------------
