@@ -310,14 +310,18 @@ def run_ours(args):
 
         e2e_step()
         barrier(world)
+        tm.reset_match_stats()
         t0 = time.perf_counter()
         e2e_steps = max(1, min(args.steps, 3))
         for _ in range(e2e_steps):
             e2e_step()
         dt = (time.perf_counter() - t0) / e2e_steps
         dt = max_over_ranks(dt, world, device="cuda")
-        line["e2e"] = {"value": round(world * e2e_nq / dt, 1), "unit": UNIT, "h2d_bytes_per_step": e2e_nq * 24,
-                       "d2h_bytes_per_step": int((e2e_nq + 1) * 8 + nk.value * 4), "queries_per_step": e2e_nq,
+        est = tm.match_stats()
+        line["e2e"] = {"value": round(world * e2e_nq / dt, 1), "unit": UNIT,
+                       "h2d_bytes_per_step": int(est["h2d_bytes"] // e2e_steps),
+                       "d2h_bytes_per_step": int(est["d2h_bytes"] // e2e_steps), "queries_per_step": e2e_nq,
+                       "keys_per_step": int(nk.value),
                        "api": "tm_match_batch (pinned host input and output buffers)"}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(f, ko, k, q, args.cpu_seconds)

@@ -173,6 +173,8 @@ typedef struct {
     double match_kernel_ms;
     uint64_t dense_tests; /* sum over batches and partitions of routed queries x partition size */
     uint64_t kernel_launches; /* all kernels launched by the matcher */
+    uint64_t h2d_bytes, d2h_bytes; /* bytes copied by tm_match_batch (keys travel as 16 bits
+                                      when every key of the table is below 65,536) */
 } tm_match_stats;
 int tm_get_match_stats(tm_engine *e, tm_match_stats *st);
 int tm_reset_match_stats(tm_engine *e);

@@ -226,6 +226,8 @@ int tm_get_match_stats(tm_engine *e, tm_match_stats *st) {
     st->match_kernel_ms = s.match_ms;
     st->dense_tests = s.dense;
     st->kernel_launches = s.launches;
+    st->h2d_bytes = s.h2d_bytes;
+    st->d2h_bytes = s.d2h_bytes;
     return TM_OK;
 }
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <immintrin.h>
 
 namespace tmb {
 
@@ -405,12 +406,54 @@ void parallel_copy(void *dst, const void *src, size_t bytes) {
     for (auto &x : th) x.join();
 }
 
+// widen 16-bit keys into the caller's 32-bit buffer: AVX2 with streaming
+// stores where the CPU has it (no read-for-ownership of the destination),
+// split over threads
+__attribute__((target("avx2"))) void widen_avx2(uint32_t *d, const uint16_t *s_, uint64_t n) {
+    uint64_t i = 0;
+    while (i < n && (reinterpret_cast<uintptr_t>(d + i) & 31)) {
+        d[i] = s_[i];
+        ++i;
+    }
+    for (; i + 8 <= n; i += 8) {
+        const __m128i v = _mm_loadu_si128(reinterpret_cast<const __m128i *>(s_ + i));
+        _mm256_stream_si256(reinterpret_cast<__m256i *>(d + i), _mm256_cvtepu16_epi32(v));
+    }
+    for (; i < n; ++i) d[i] = s_[i];
+    _mm_sfence();
+}
+
+void widen_scalar(uint32_t *d, const uint16_t *s_, uint64_t n) {
+    for (uint64_t i = 0; i < n; ++i) d[i] = s_[i];
+}
+
+void parallel_widen(uint32_t *dst, const uint16_t *src, uint64_t n) {
+    static const bool avx2 = __builtin_cpu_supports("avx2");
+    void (*body)(uint32_t *, const uint16_t *, uint64_t) = avx2 ? widen_avx2 : widen_scalar;
+    const uint64_t kMin = uint64_t(8) << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = int(std::min<uint64_t>(std::max(1u, hw - 2), std::max<uint64_t>(1, n / kMin)));
+    if (nt == 1) {
+        body(dst, src, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    const uint64_t per = ((n + nt - 1) / nt + 7) & ~uint64_t(7);
+    for (int t = 0; t < nt; ++t) {
+        const uint64_t b = uint64_t(t) * per, e = std::min(n, b + per);
+        if (b < e) th.emplace_back(body, dst + b, src + b, e - b);
+    }
+    for (auto &x : th) x.join();
+}
+
 }  // namespace
 
 // Batches alternate between two lanes (scratch + stream + pinned staging):
 // while one batch's results travel to the host, the next batch is matched.
 // Keys go straight into a pinned caller buffer; a pageable one is filled
-// from pinned staging by copy threads.
+// from pinned staging by copy threads.  When every key of the table is
+// below 65,536 the keys cross PCIe as 16-bit values and copy threads widen
+// them into the caller's buffer (half the bytes on the link).
 void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
                         uint64_t capacity, uint64_t *n_keys) {
     std::lock_guard<std::mutex> lk(api_mtx_);
@@ -425,7 +468,9 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     cudaStream_t str[2] = {d.stream, d.stream2};
     HostBuf<uint64_t> *hoff[2] = {&d.h_offsets, &d.h_offsets2};
     HostBuf<uint32_t> *hkeys[2] = {&d.h_keys, &d.h_keys2};
-    const bool direct = out_keys != nullptr && is_pinned(out_keys);
+    HostBuf<uint16_t> *hk16[2] = {&d.h_keys16, &d.h_keys16b};
+    const bool narrow = d.table.max_key < 65536u;
+    const bool direct = !narrow && out_keys != nullptr && is_pinned(out_keys);
     struct Pending {
         bool active = false;
         uint64_t q0 = 0, base = 0, nk = 0;
@@ -461,6 +506,8 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             sc.profile = profile_;
             match_batch(d.table, sc.queries.p, n, unique, sc, &doff, &dkeys, &nk, &bs, str[l]);
             stats_.add(bs, n, profile_);
+            stats_.h2d_bytes += uint64_t(n) * 24;
+            stats_.d2h_bytes += (uint64_t(n) + 1) * 8 + nk * (narrow ? 2 : 4);
             hoff[l]->reserve(size_t(n) + 1);
             TM_CUDA(cudaMemcpyAsync(hoff[l]->p, doff, (size_t(n) + 1) * 8, cudaMemcpyDeviceToHost, str[l]));
             Pending &p = pend[l];
@@ -471,7 +518,19 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             p.nk = nk;
             p.staged = false;
             if (!overflow && total + nk <= capacity) {
-                if (nk && direct) {
+                if (nk && narrow) {
+                    const uint16_t *d16 = narrow_keys(dkeys, nk, sc, str[l]);
+                    hk16[l]->reserve(nk);
+                    TM_CUDA(cudaMemcpyAsync(hk16[l]->p, d16, nk * 2, cudaMemcpyDeviceToHost, str[l]));
+                    TM_CUDA(cudaEventRecord(d.lane_done[l], str[l]));
+                    p.staged = true;
+                    cudaEvent_t ev = d.lane_done[l];
+                    uint32_t *dst = out_keys + total;
+                    const uint16_t *src = hk16[l]->p;
+                    p.copier = std::thread([=] {
+                        if (cudaEventSynchronize(ev) == cudaSuccess) parallel_widen(dst, src, nk);
+                    });
+                } else if (nk && direct) {
                     TM_CUDA(cudaMemcpyAsync(out_keys + total, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
                 } else if (nk) {
                     hkeys[l]->reserve(nk);

@@ -60,6 +60,7 @@ struct EngineStats {
     uint64_t match_launches = 0;
     double match_ms = 0.0;
     uint64_t dense = 0, launches = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;  // host API transfers
     void add(const BatchStats &b, uint32_t nq, bool profiled) {
         batches++;
         queries += nq;
@@ -145,6 +146,7 @@ private:
         HostBuf<uint32_t> h_queries;
         HostBuf<uint64_t> h_offsets, h_offsets2;
         HostBuf<uint32_t> h_keys, h_keys2;
+        HostBuf<uint16_t> h_keys16, h_keys16b;
         std::thread worker;
     };
     void build_device_table(Device &d);

@@ -54,6 +54,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     chunk_off = std::move(o.chunk_off);
     slices = std::move(o.slices);
     work = std::move(o.work);
+    keys16 = std::move(o.keys16);
     counters = std::move(o.counters);
     pairs = std::move(o.pairs);
     qkeys = std::move(o.qkeys);
@@ -73,6 +74,16 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     ev_end = o.ev_end;
     o.ev_begin = o.ev_end = nullptr;
     return *this;
+}
+
+const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s, cudaStream_t st) {
+    s.keys16.reserve(std::max<uint64_t>(n, 1) + 8);
+    if (n) {
+        const unsigned blocks = unsigned(std::min<uint64_t>((n / 4 + 255) / 256 + 1, 148 * 16));
+        k_narrow16<<<blocks, 256, 0, st>>>(d_keys, n, s.keys16.p);
+        TM_CHECK_LAUNCH();
+    }
+    return s.keys16.p;
 }
 
 MatchScratch::~MatchScratch() {

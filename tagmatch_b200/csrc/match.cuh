@@ -19,6 +19,7 @@ struct MatchScratch {
     DevBuf<uint32_t> chunk_off;   // [P + 1] 256-query chunks per partition (prefix)
     DevBuf<uint32_t> slices;      // [chunks][192][8] bit-sliced "lacks bit" masks
     DevBuf<unsigned long long> work;  // optional kernel work counters
+    DevBuf<uint16_t> keys16;          // keys narrowed for the host transfer
     DevBuf<unsigned long long> counters;  // [0] work item, [1] pairs, [2] error flags
     DevBuf<Pair> pairs;
     DevBuf<uint32_t> qkeys;       // [nq]
@@ -61,6 +62,9 @@ struct BatchStats {
 void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, MatchScratch &s,
                  const uint64_t **d_offsets, const uint32_t **d_keys, uint64_t *n_keys, BatchStats *stats,
                  cudaStream_t st, cudaEvent_t match_begin = nullptr, cudaEvent_t match_end = nullptr);
+
+// Narrows n keys (all < 65,536) to 16 bits into s.keys16 on stream st.
+const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s, cudaStream_t st);
 
 // The same pipeline with all scratch in a static device array (noalloc.cu).
 void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_out_offsets,

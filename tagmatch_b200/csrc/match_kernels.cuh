@@ -575,5 +575,22 @@ __global__ void k_compact(const uint32_t *__restrict__ ukeys, const uint64_t *__
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) out[dst + i] = ukeys[src + i];
 }
 
+// Keys narrowed to 16 bits for the trip to the host (tables whose largest
+// key is below 65,536); the host widens them back.
+__global__ void k_narrow16(const uint32_t *__restrict__ in, uint64_t n, uint16_t *__restrict__ out) {
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i * 4 < n; i += stride) {
+        if (i * 4 + 4 <= n && (reinterpret_cast<uintptr_t>(in) & 15) == 0) {
+            const uint4 v = reinterpret_cast<const uint4 *>(in)[i];
+            uint2 w;
+            w.x = (v.x & 0xFFFFu) | (v.y << 16);
+            w.y = (v.z & 0xFFFFu) | (v.w << 16);
+            reinterpret_cast<uint2 *>(out)[i] = w;
+        } else {
+            for (uint64_t k = i * 4; k < n && k < i * 4 + 4; ++k) out[k] = uint16_t(in[k]);
+        }
+    }
+}
+
 }  // namespace
 }  // namespace tmb
