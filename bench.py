@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rates", default="200000,500000,1000000")
+    ap.add_argument("--serve-seconds", type=float, default=4.0)
     return ap.parse_args()
 
 
@@ -182,6 +185,21 @@ def cpu_baseline(f, ko, k, q, seconds):
     return {"value": m / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"first {m} of the step's queries against the full {f.shape[0]}-filter table "
                       f"(oracle/oracle.c restatement of test_matcher.cc:74-81), {dt:.1f} s"}
+
+
+def serving(args):
+    """Latency under a Poisson load of 1..4096-query requests (C++ driver over
+    tm_submit): plain = one request per device batch, continuous = pending
+    requests share batches on two lanes."""
+    from tagmatch_b200 import build
+    cmd = [build.SERVE_BENCH, f"filters={args.filters}", "pool=1048576", f"seed={SEED}", f"maxp={MAX_P}",
+           f"rates={args.serve_rates}", "modes=plain,continuous", f"seconds={args.serve_seconds}"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        return {"error": out.stderr[-500:]}
+    runs = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    return {"workload": "Poisson arrivals, request sizes log-uniform 1..4096 queries, 10M-filter table, match",
+            "runs": runs}
 
 
 def run_ours(args):
@@ -325,6 +343,8 @@ def run_ours(args):
                        "api": "tm_match_batch (pinned host input and output buffers)"}
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(f, ko, k, q, args.cpu_seconds)
+    if rank == 0 and world == 1 and not args.no_serve:
+        line["serving"] = serving(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     tm.close()

@@ -139,6 +139,34 @@ int tm_match_batch_device_noalloc(tm_engine *e, const uint32_t *d_queries, uint3
 int tm_match_async(tm_engine *e, const uint32_t query[TM_FILTER_WORDS], int unique, uint64_t tag, tm_match_callback cb,
                    void *user);
 
+/* Serving: a request of n queries [n][6] matched asynchronously; cb fires
+ * once, on an engine thread, with the request's results (offsets[n + 1]
+ * relative to keys) and a status.  Requests pending together are matched
+ * in shared device batches (see tm_set_flush_mode).  Extends tm_match_async
+ * (front_end.cc:540-551) from one query to a request. */
+typedef void (*tm_request_callback)(void *user, uint64_t tag, const uint64_t *offsets, const uint32_t *keys,
+                                    uint32_t n_queries, int status);
+int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uint64_t tag, tm_request_callback cb,
+              void *user);
+
+/* When pending asynchronous work goes to the device:
+ * TM_FLUSH_FULL_OR_LATENCY (default): a full batch (tm_set_batch_limit),
+ *   the latency limit, or stop() -- the reference front end's rule
+ *   (front_end.cc:325-376, 563-598);
+ * TM_FLUSH_IMMEDIATE: whenever one of the device's two lanes is free, all
+ *   pending requests (up to the batch limit and the memory budget) form the
+ *   next batch -- continuous batching;
+ * TM_FLUSH_SINGLE: one request per device batch on one lane (the plain
+ *   batched path, for comparison). */
+#define TM_FLUSH_FULL_OR_LATENCY 0
+#define TM_FLUSH_IMMEDIATE 1
+#define TM_FLUSH_SINGLE 2
+int tm_set_flush_mode(tm_engine *e, int mode);
+/* Device-memory budget per lane for a batch's queues, pairs and keys; the
+ * number of queries admitted into one batch is capped by it (estimated
+ * from the bytes per query of recent batches).  Default 16 GiB. */
+int tm_set_memory_budget(tm_engine *e, uint64_t bytes);
+
 /* partitioning::balanced_partitioning(fib, masks) -- partitioning.cc:361-411,
  * run by the GPU partitioner.  filters: n unique filters [n][6].
  * partition_of[i] receives filter i's partition id; masks[p][6] the AND of

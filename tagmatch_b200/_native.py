@@ -29,6 +29,10 @@ STATUS_NAMES = {
 u32p = ctypes.POINTER(ctypes.c_uint32)
 u64p = ctypes.POINTER(ctypes.c_uint64)
 MATCH_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64, u32p, ctypes.c_uint64)
+REQUEST_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64, u64p, u32p, ctypes.c_uint32, ctypes.c_int)
+TM_FLUSH_FULL_OR_LATENCY = 0
+TM_FLUSH_IMMEDIATE = 1
+TM_FLUSH_SINGLE = 2
 
 
 class TableInfo(ctypes.Structure):
@@ -75,6 +79,10 @@ SIGNATURES = {
                                                      ctypes.c_void_p]),
     "tm_match_async": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_int, ctypes.c_uint64, MATCH_CALLBACK,
                                       ctypes.c_void_p]),
+    "tm_submit": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, REQUEST_CALLBACK,
+                                 ctypes.c_void_p]),
+    "tm_set_flush_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tm_set_memory_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "tm_balanced_partitioning": (ctypes.c_int, [u32p, ctypes.c_uint64, ctypes.c_uint32, u32p, u32p, u32p,
                                                 ctypes.c_uint64, u64p]),
     "tm_get_table_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableInfo)]),

@@ -7,6 +7,7 @@ Outputs (next to this file):
   libtagmatch_b200.so   engine, CUDA kernels (sm_100a) and the C ABI
   libtm_workload.so     seeded workload generator (CPU)
   tagmatch_facade_test  C++ facade test driver (tagmatch.hh-compatible API)
+  tagmatch_serve_bench  serving load generator over the C ABI (tm_submit)
 """
 import os
 import subprocess
@@ -27,6 +28,7 @@ HEADERS = ["tm_device.cuh", "tm_host.hpp", "scan.cuh", "partition.cuh", "match.c
 LIB = os.path.join(HERE, "libtagmatch_b200.so")
 WORKLOAD_LIB = os.path.join(HERE, "libtm_workload.so")
 FACADE_TEST = os.path.join(HERE, "tagmatch_facade_test")
+SERVE_BENCH = os.path.join(HERE, "tagmatch_serve_bench")
 
 
 def _run(cmd):
@@ -72,6 +74,15 @@ def build_facade_test(quick=False):
     return FACADE_TEST
 
 
+def build_serve_bench(quick=False):
+    srcs = [os.path.join(CSRC, "serve_bench.cc"), os.path.join(CSRC, "workload.cc")]
+    if quick and not _stale(SERVE_BENCH, srcs + [LIB]):
+        return SERVE_BENCH
+    _run([CXX, "-O2", "-std=c++17", "-I" + INCLUDE, "-o", SERVE_BENCH, *srcs,
+          "-L" + HERE, "-ltagmatch_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+    return SERVE_BENCH
+
+
 def build_oracle():
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
 
@@ -80,6 +91,7 @@ def build_all(quick=False):
     build_workload(quick)
     build_engine(quick)
     build_facade_test(quick)
+    build_serve_bench(quick)
 
 
 if __name__ == "__main__":

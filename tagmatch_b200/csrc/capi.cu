@@ -155,6 +155,24 @@ int tm_match_async(tm_engine *e, const uint32_t query[TM_FILTER_WORDS], int uniq
     });
 }
 
+int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uint64_t tag, tm_request_callback cb,
+              void *user) {
+    if (!e || (n && !queries) || !cb) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.submit_request(queries, n, unique != 0, tag, cb, user); });
+}
+
+int tm_set_flush_mode(tm_engine *e, int mode) {
+    if (!e || mode < TM_FLUSH_FULL_OR_LATENCY || mode > TM_FLUSH_SINGLE) return TM_ERR_INVALID;
+    e->eng.set_flush_mode(mode);
+    return TM_OK;
+}
+
+int tm_set_memory_budget(tm_engine *e, uint64_t bytes) {
+    if (!e || bytes == 0) return TM_ERR_INVALID;
+    e->eng.set_memory_budget(bytes);
+    return TM_OK;
+}
+
 int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p, uint32_t *partition_of,
                              uint32_t *masks, uint32_t *sizes, uint64_t capacity, uint64_t *n_partitions) {
     if ((n && (!filters || !partition_of)) || !n_partitions || max_p == 0) return TM_ERR_INVALID;

@@ -35,6 +35,8 @@ Engine::~Engine() {
         cudaSetDevice(d->id);
         if (d->stream) cudaStreamDestroy(d->stream);
         if (d->stream2) cudaStreamDestroy(d->stream2);
+        for (auto &ln : d->lanes)
+            if (ln.stream) cudaStreamDestroy(ln.stream);
         for (cudaEvent_t ev : d->lane_done)
             if (ev) cudaEventDestroy(ev);
     }
@@ -220,7 +222,14 @@ void Engine::start(uint32_t threads, uint32_t gpus) {
         flush_now_ = false;
         if (!pending_.empty()) oldest_ = std::chrono::steady_clock::now();
     }
-    for (uint32_t g = 0; g < gpus_; ++g) devs_[g]->worker = std::thread(&Engine::worker_loop, this, int(g));
+    for (uint32_t g = 0; g < gpus_; ++g) {
+        Device &d = *devs_[g];
+        TM_CUDA(cudaSetDevice(d.id));
+        for (int l = 0; l < kLanes; ++l) {
+            if (!d.lanes[l].stream) TM_CUDA(cudaStreamCreateWithFlags(&d.lanes[l].stream, cudaStreamNonBlocking));
+            d.lanes[l].th = std::thread(&Engine::worker_loop, this, int(g), l);
+        }
+    }
 }
 
 void Engine::stop() {
@@ -231,7 +240,8 @@ void Engine::stop() {
     }
     q_cv_.notify_all();
     for (auto &d : devs_)
-        if (d->worker.joinable()) d->worker.join();
+        for (auto &ln : d->lanes)
+            if (ln.th.joinable()) ln.th.join();
     std::lock_guard<std::mutex> ql(q_mtx_);
     started_ = false;
     stopping_ = false;
@@ -252,30 +262,72 @@ void Engine::clear() {
         d->table = DevTable();
         d->scratch = MatchScratch();
         d->scratch2 = MatchScratch();
+        for (auto &ln : d->lanes) ln.scratch = MatchScratch();
         d->table_ready = false;
     }
 }
 
-void Engine::submit(const AsyncRequest &r) {
+void Engine::enqueue(RequestPtr r) {
     {
         std::lock_guard<std::mutex> ql(q_mtx_);
         if (pending_.empty()) oldest_ = std::chrono::steady_clock::now();
-        pending_.push_back(r);
+        pending_queries_ += r->n;
+        pending_.push_back(std::move(r));
     }
-    q_cv_.notify_one();
+    q_cv_.notify_all();
 }
 
-void Engine::worker_loop(int dev) {
+void Engine::submit(const AsyncRequest &a) {
+    auto r = std::make_shared<Request>();
+    r->words.assign(a.words, a.words + kWords);
+    r->n = 1;
+    r->unique = a.unique;
+    r->tag = a.tag;
+    r->qcb = a.cb;
+    r->user = a.user;
+    enqueue(std::move(r));
+}
+
+void Engine::submit_request(const uint32_t *queries, uint32_t n, bool unique, uint64_t tag, BatchCallback bcb, void *user) {
+    auto r = std::make_shared<Request>();
+    r->words.assign(queries, queries + size_t(n) * kWords);
+    r->n = n;
+    r->unique = unique;
+    r->tag = tag;
+    r->bcb = bcb;
+    r->user = user;
+    if (n == 0) {  // nothing to match: complete at once
+        const uint64_t zero = 0;
+        if (bcb) bcb(user, tag, &zero, nullptr, 0, TM_OK);
+        return;
+    }
+    enqueue(std::move(r));
+}
+
+// One lane of the asynchronous matcher.  It takes pending requests (or
+// pieces of them, up to the batch limit and to the queries that fit the
+// device-memory budget), matches them as one device batch on its own
+// stream, and completes them.  Two lanes per device keep one batch on the
+// GPU while the other is staged or delivered.
+void Engine::worker_loop(int dev, int lane) {
     Device &d = *devs_[dev];
+    Lane &ln = d.lanes[lane];
     cudaSetDevice(d.id);
-    std::vector<AsyncRequest> batch;
+    std::vector<Piece> pieces;
     for (;;) {
-        batch.clear();
+        pieces.clear();
+        bool unique = false;
+        uint32_t total = 0;
         {
             std::unique_lock<std::mutex> lk(q_mtx_);
             for (;;) {
+                const int mode = flush_mode_.load();
+                if (mode == kFlushSingle && lane != 0 && !stopping_) {
+                    q_cv_.wait(lk);  // the plain path uses one lane
+                    continue;
+                }
                 if (!pending_.empty()) {
-                    if (stopping_ || flush_now_ || pending_.size() >= batch_limit_) break;
+                    if (stopping_ || flush_now_ || mode != kFlushFullOrLatency || pending_queries_ >= batch_limit_) break;
                     const uint32_t lim = latency_ms_.load();
                     if (lim > 0) {
                         auto due = oldest_ + std::chrono::milliseconds(lim);
@@ -288,62 +340,112 @@ void Engine::worker_loop(int dev) {
                 }
                 q_cv_.wait(lk);
             }
-            const size_t take = std::min<size_t>(pending_.size(), batch_limit_);
-            for (size_t i = 0; i < take; ++i) {
-                batch.push_back(pending_.front());
-                pending_.pop_front();
+            const int mode = flush_mode_.load();
+            const uint64_t budget_q = std::max<uint64_t>(1, memory_budget_.load() / std::max<uint64_t>(1, bytes_per_query_.load()));
+            const uint32_t cap = uint32_t(std::min<uint64_t>(batch_limit_, budget_q));
+            unique = pending_.front()->unique;
+            while (!pending_.empty() && total < cap) {
+                RequestPtr &r = pending_.front();
+                if (r->unique != unique) break;
+                // a request is split over batches only when it alone exceeds
+                // the cap; otherwise it waits for the next batch
+                if (total > 0 && r->taken == 0 && r->n > cap - total) break;
+                const uint32_t take = std::min(r->n - r->taken, cap - total);
+                pieces.push_back(Piece{r, r->taken, take});
+                r->taken += take;
+                total += take;
+                if (r->taken == r->n) pending_.pop_front();
+                if (mode == kFlushSingle) break;
             }
+            pending_queries_ -= total;
             if (!pending_.empty()) oldest_ = std::chrono::steady_clock::now();
-            in_flight_ += batch.size();
+            in_flight_ += total;
         }
-        run_async_batch(d, batch);
+        run_pieces(d, ln, pieces, unique);
         {
             std::lock_guard<std::mutex> lk(q_mtx_);
-            in_flight_ -= batch.size();
+            in_flight_ -= total;
         }
         done_cv_.notify_all();
+        q_cv_.notify_all();
     }
 }
 
-void Engine::run_async_batch(Device &d, std::vector<AsyncRequest> &batch) {
-    // match and match_unique requests of one batch run as two sub-batches
-    for (int u = 0; u < 2; ++u) {
-        std::vector<size_t> idx;
-        for (size_t i = 0; i < batch.size(); ++i)
-            if (batch[i].unique == (u == 1)) idx.push_back(i);
-        if (idx.empty()) continue;
-        const uint32_t nq = uint32_t(idx.size());
-        bool ok = true;
-        try {
-            d.h_queries.reserve(size_t(nq) * kWords);
-            for (uint32_t i = 0; i < nq; ++i) std::memcpy(d.h_queries.p + size_t(i) * kWords, batch[idx[i]].words, 24);
-            d.scratch.queries.reserve(size_t(nq) * kWords);
-            TM_CUDA(cudaMemcpyAsync(d.scratch.queries.p, d.h_queries.p, size_t(nq) * 24, cudaMemcpyHostToDevice, d.stream));
-            const uint64_t *doff;
-            const uint32_t *dkeys;
-            uint64_t nk = 0;
-            BatchStats bs;
-            match_batch(d.table, d.scratch.queries.p, nq, u == 1, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
-            d.h_offsets.reserve(size_t(nq) + 1);
-            d.h_keys.reserve(std::max<uint64_t>(nk, 1));
-            TM_CUDA(cudaMemcpyAsync(d.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, d.stream));
-            if (nk) TM_CUDA(cudaMemcpyAsync(d.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, d.stream));
-            TM_CUDA(cudaStreamSynchronize(d.stream));
-        } catch (const Error &e) {
-            ok = false;
-            std::lock_guard<std::mutex> lk(q_mtx_);
-            async_error_ = e.what();
+void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool unique) {
+    uint32_t nq = 0;
+    for (const Piece &p : pieces) nq += p.n;
+    bool ok = true;
+    try {
+        ln.h_queries.reserve(size_t(nq) * kWords);
+        uint32_t at = 0;
+        for (const Piece &p : pieces) {
+            std::memcpy(ln.h_queries.p + size_t(at) * kWords, p.r->words.data() + size_t(p.q0) * kWords,
+                        size_t(p.n) * kWords * sizeof(uint32_t));
+            at += p.n;
         }
-        for (uint32_t i = 0; i < nq; ++i) {
-            const AsyncRequest &r = batch[idx[i]];
-            if (!r.cb) continue;
+        ln.scratch.queries.reserve(size_t(nq) * kWords);
+        TM_CUDA(cudaMemcpyAsync(ln.scratch.queries.p, ln.h_queries.p, size_t(nq) * 24, cudaMemcpyHostToDevice, ln.stream));
+        const uint64_t *doff;
+        const uint32_t *dkeys;
+        uint64_t nk = 0;
+        BatchStats bs;
+        match_batch(d.table, ln.scratch.queries.p, nq, unique, ln.scratch, &doff, &dkeys, &nk, &bs, ln.stream);
+        ln.h_offsets.reserve(size_t(nq) + 1);
+        ln.h_keys.reserve(std::max<uint64_t>(nk, 1));
+        TM_CUDA(cudaMemcpyAsync(ln.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, ln.stream));
+        if (nk) TM_CUDA(cudaMemcpyAsync(ln.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, ln.stream));
+        TM_CUDA(cudaStreamSynchronize(ln.stream));
+        // running estimate of device bytes per query (queues, pairs, keys)
+        const uint64_t bytes = bs.routed * (kQueueWords * 4) + bs.pairs * sizeof(Pair) + nk * 4 * (unique ? 3 : 1);
+        const uint64_t bpq = std::max<uint64_t>(1024, bytes / std::max<uint32_t>(nq, 1));
+        bytes_per_query_.store((bytes_per_query_.load() * 3 + bpq) / 4);
+    } catch (const Error &e) {
+        ok = false;
+        std::lock_guard<std::mutex> lk(q_mtx_);
+        async_error_ = e.what();
+    }
+    const uint64_t *off = ln.h_offsets.p;
+    const uint32_t *keys = ln.h_keys.p;
+    uint32_t at = 0;
+    std::vector<uint64_t> rebased;
+    for (Piece &p : pieces) {
+        Request &r = *p.r;
+        if (r.qcb) {
+            for (uint32_t i = 0; i < p.n; ++i) {
+                if (ok) r.qcb(r.user, r.tag + p.q0 + i, keys + off[at + i], off[at + i + 1] - off[at + i]);
+                else r.qcb(r.user, r.tag + p.q0 + i, nullptr, 0);
+            }
+        } else if (r.bcb && p.q0 == 0 && p.n == r.n) {
+            // whole request in this batch: offsets rebased to its first key
+            rebased.resize(size_t(p.n) + 1);
+            const uint64_t b0 = ok ? off[at] : 0;
+            for (uint32_t i = 0; i <= p.n; ++i) rebased[i] = ok ? off[at + i] - b0 : 0;
+            r.bcb(r.user, r.tag, rebased.data(), ok ? keys + b0 : nullptr, r.n, ok ? TM_OK : TM_ERR_INTERNAL);
+        } else if (r.bcb) {
+            // a piece of a split request: keep it until every piece is in
+            std::lock_guard<std::mutex> rl(r.mtx);
+            if (r.counts.empty()) {
+                r.counts.assign(r.n, 0);
+                r.part.resize(r.n);
+            }
             if (ok) {
-                const uint64_t b = d.h_offsets.p[i], e = d.h_offsets.p[i + 1];
-                r.cb(r.user, r.tag, d.h_keys.p + b, e - b);
+                for (uint32_t i = 0; i < p.n; ++i) r.counts[p.q0 + i] = uint32_t(off[at + i + 1] - off[at + i]);
+                r.part[p.q0].assign(keys + off[at], keys + off[at + p.n]);
             } else {
-                r.cb(r.user, r.tag, nullptr, 0);
+                r.status = TM_ERR_INTERNAL;
+            }
+            r.done += p.n;
+            if (r.done == r.n) {
+                std::vector<uint64_t> o(size_t(r.n) + 1, 0);
+                for (uint32_t i = 0; i < r.n; ++i) o[i + 1] = o[i] + r.counts[i];
+                std::vector<uint32_t> all;
+                all.reserve(o[r.n]);
+                for (uint32_t q = 0; q < r.n; ++q)
+                    if (!r.part[q].empty()) all.insert(all.end(), r.part[q].begin(), r.part[q].end());
+                r.bcb(r.user, r.tag, o.data(), all.data(), r.n, r.status);
             }
         }
+        at += p.n;
     }
 }
 

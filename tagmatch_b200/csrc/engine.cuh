@@ -45,6 +45,8 @@ struct KeysetChange {
 };
 
 typedef void (*MatchCallback)(void *user, uint64_t tag, const uint32_t *keys, uint64_t n_keys);
+typedef void (*BatchCallback)(void *user, uint64_t tag, const uint64_t *offsets, const uint32_t *keys, uint32_t n_queries,
+                              int status);
 
 struct AsyncRequest {
     uint32_t words[kWords];
@@ -52,6 +54,33 @@ struct AsyncRequest {
     uint64_t tag;
     MatchCallback cb;
     void *user;
+};
+
+// A submitted request of n queries, completed either per query (qcb,
+// match_handler semantics) or as a whole (bcb).
+struct Request {
+    std::vector<uint32_t> words;  // [n][6]
+    uint32_t n = 0;
+    bool unique = false;
+    uint64_t tag = 0;
+    MatchCallback qcb = nullptr;
+    BatchCallback bcb = nullptr;
+    void *user = nullptr;
+    uint32_t taken = 0;  // queries placed in device batches (queue lock)
+    // pieces of a request split over several device batches
+    std::mutex mtx;
+    uint32_t done = 0;
+    int status = 0;
+    std::vector<uint32_t> counts;             // keys per query
+    std::vector<std::vector<uint32_t>> part;  // keys per piece, by first query
+};
+using RequestPtr = std::shared_ptr<Request>;
+
+// When asynchronous batches go to the device.
+enum FlushMode : int {
+    kFlushFullOrLatency = 0,  // full batch, latency limit, or stop() (front_end.cc semantics)
+    kFlushImmediate = 1,      // whenever a lane is free: continuous batching of all pending requests
+    kFlushSingle = 2,         // one request per device batch, one lane (plain batched path)
 };
 
 struct EngineStats {
@@ -118,6 +147,10 @@ public:
     // asynchronous match: cb fires exactly once per request, on an engine
     // thread, after start() (requests made earlier wait for it)
     void submit(const AsyncRequest &r);
+    // request of n queries [n][6]; bcb fires once with all its results
+    void submit_request(const uint32_t *queries, uint32_t n, bool unique, uint64_t tag, BatchCallback bcb, void *user);
+    void set_flush_mode(int m) { flush_mode_.store(m); }
+    void set_memory_budget(uint64_t bytes) { memory_budget_.store(bytes ? bytes : 1); }
 
     // table introspection
     uint32_t n_filters() const { return uint32_t(key_off_.size() ? key_off_.size() - 1 : 0); }
@@ -136,6 +169,19 @@ public:
     const std::vector<uint32_t> &keys() const { return keys_; }
 
 private:
+    static constexpr int kLanes = 2;
+    struct Lane {
+        MatchScratch scratch;
+        cudaStream_t stream = nullptr;
+        HostBuf<uint32_t> h_queries;
+        HostBuf<uint64_t> h_offsets;
+        HostBuf<uint32_t> h_keys;
+        std::thread th;
+    };
+    struct Piece {
+        RequestPtr r;
+        uint32_t q0, n;
+    };
     struct Device {
         int id = 0;
         cudaStream_t stream = nullptr, stream2 = nullptr;
@@ -147,12 +193,13 @@ private:
         HostBuf<uint64_t> h_offsets, h_offsets2;
         HostBuf<uint32_t> h_keys, h_keys2;
         HostBuf<uint16_t> h_keys16, h_keys16b;
-        std::thread worker;
+        Lane lanes[kLanes];  // asynchronous matcher lanes
     };
     void build_device_table(Device &d);
     Device &device(int i);
-    void worker_loop(int dev);
-    void run_async_batch(Device &d, std::vector<AsyncRequest> &batch);
+    void enqueue(RequestPtr r);
+    void worker_loop(int dev, int lane);
+    void run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool unique);
 
     std::map<FilterKey, KeysetChange> updates_;
     bool already_consolidated_ = false;
@@ -177,7 +224,11 @@ private:
     // async path
     std::mutex q_mtx_;
     std::condition_variable q_cv_, done_cv_;
-    std::deque<AsyncRequest> pending_;
+    std::deque<RequestPtr> pending_;
+    uint64_t pending_queries_ = 0;
+    std::atomic<int> flush_mode_{kFlushFullOrLatency};
+    std::atomic<uint64_t> memory_budget_{uint64_t(16) << 30};  // per lane
+    std::atomic<uint64_t> bytes_per_query_{64 << 10};         // running estimate
     std::chrono::steady_clock::time_point oldest_;
     uint64_t in_flight_ = 0;
     bool started_ = false, stopping_ = false, flush_now_ = false;

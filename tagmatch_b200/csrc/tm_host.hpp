@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <algorithm>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -50,8 +51,11 @@ struct DevBuf {
         return *this;
     }
     ~DevBuf() { release(); }
+    // Grows by at least half the current capacity, so a slowly growing
+    // demand reallocates (and frees, which synchronises the device) rarely.
     void reserve(size_t n) {
         if (n <= cap && p) return;
+        if (p) n = std::max(n, cap + cap / 2);
         release();
         size_t bytes = (n ? n : 1) * sizeof(T);
         cudaError_t e = cudaMalloc(&p, bytes);
@@ -83,6 +87,7 @@ struct HostBuf {
     ~HostBuf() { release(); }
     void reserve(size_t n) {
         if (n <= cap && p) return;
+        if (p) n = std::max(n, cap + cap / 2);
         release();
         size_t bytes = (n ? n : 1) * sizeof(T);
         cudaError_t e = cudaMallocHost(&p, bytes);

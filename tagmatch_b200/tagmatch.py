@@ -79,6 +79,7 @@ class TagMatch:
         self._cb_lock = threading.Lock()
         self._next_tag = 1
         self._cfunc = _native.MATCH_CALLBACK(self._on_done)
+        self._rfunc = _native.REQUEST_CALLBACK(self._on_request)
 
     # -- plumbing --------------------------------------------------------
     def _check(self, st, h=None):
@@ -188,6 +189,37 @@ class TagMatch:
                 self._callbacks.pop(tag, None)
             self._check(st)
         return tag
+
+    def submit(self, queries, handler, unique=False):
+        """Queues a request of n queries; handler(offsets, keys, status) runs
+        once, on an engine thread, with the request's results."""
+        q = as_filters(queries)
+        with self._cb_lock:
+            tag = self._next_tag
+            self._next_tag += 1
+            self._callbacks[tag] = handler
+        st = self._lib.tm_submit(self._h, _p32(q) if q.shape[0] else None, q.shape[0], 1 if unique else 0, tag,
+                                 self._rfunc, None)
+        if st != _native.TM_OK:
+            with self._cb_lock:
+                self._callbacks.pop(tag, None)
+            self._check(st)
+        return tag
+
+    def set_flush_mode(self, mode):
+        self._check(self._lib.tm_set_flush_mode(self._h, mode))
+
+    def set_memory_budget(self, nbytes):
+        self._check(self._lib.tm_set_memory_budget(self._h, nbytes))
+
+    def _on_request(self, user, tag, offsets, keys, n, status):
+        off = np.ctypeslib.as_array(offsets, shape=(n + 1,)).copy()
+        nk = int(off[-1])
+        arr = np.ctypeslib.as_array(keys, shape=(nk,)).copy() if nk else np.zeros(0, dtype=np.uint32)
+        with self._cb_lock:
+            h = self._callbacks.pop(tag, None)
+        if h is not None:
+            h(off, arr, status)
 
     def match_unique(self, query, handler):
         return self.match(query, handler, unique=True)

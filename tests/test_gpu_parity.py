@@ -270,3 +270,62 @@ def test_config1_table_sampled_parity():
     for i in range(0, 20000, 97):
         assert np.array_equal(np.unique(keys[off[i]:off[i + 1]]), ukeys[uoff[i]:uoff[i + 1]])
     tm.close()
+
+
+@pytest.mark.parametrize("mode", [_native.TM_FLUSH_IMMEDIATE, _native.TM_FLUSH_SINGLE, _native.TM_FLUSH_FULL_OR_LATENCY])
+def test_submit_requests_same_alone_and_mixed(mode):
+    """Serving: requests of 1..700 queries, merged into shared device batches
+    (or one per batch), split across batches when the batch limit is small;
+    each request's result equals the same queries matched alone."""
+    f, ko, k = workload.generate_filters(30000, 44)
+    q = workload.generate_queries(3000, f, 44)
+    tm = engine_with(f, ko, k, 4096)
+    rng = np.random.default_rng(5)
+    reqs, at = [], 0
+    while at < q.shape[0]:
+        n = int(min(q.shape[0] - at, rng.integers(1, 700)))
+        reqs.append((at, n, bool(rng.integers(0, 2))))
+        at += n
+    expect = {}
+    for i, (a, n, u) in enumerate(reqs):
+        expect[i] = tm.match_batch(q[a:a + n], unique=u)
+    got = {}
+    lock = threading.Lock()
+
+    def handler(i):
+        def h(off, keys, status):
+            with lock:
+                assert i not in got
+                got[i] = (off, keys, status)
+        return h
+
+    tm.set_flush_mode(mode)
+    tm.set_batch_limit(1000)  # forces merging and splitting
+    tm.set_latency_limit_ms(2)
+    tm.start(4, 1)
+    for i, (a, n, u) in enumerate(reqs):
+        tm.submit(q[a:a + n], handler(i), unique=u)
+    tm.stop()
+    assert len(got) == len(reqs)
+    for i, (a, n, u) in enumerate(reqs):
+        off, keys, status = got[i]
+        eoff, ekeys = expect[i]
+        assert status == 0
+        assert np.array_equal(off, eoff)
+        if u:
+            assert np.array_equal(keys, ekeys)
+        else:
+            assert_same_multisets(off, keys, eoff, ekeys)
+    tm.close()
+
+
+def test_serve_bench_runs():
+    """The serving load generator completes every request in both modes."""
+    import json
+    out = subprocess.run([build.SERVE_BENCH, "filters=200000", "pool=65536", "rates=20000", "seconds=1"],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+    assert {l["mode"] for l in lines} == {"plain", "continuous"}
+    for l in lines:
+        assert l["requests"] > 0 and l["p99_ms"] >= l["p50_ms"] > 0
