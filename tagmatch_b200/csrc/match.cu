@@ -165,7 +165,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     s.chunk_off.reserve(size_t(P) + 1);
     TM_CUDA(cudaMemcpyAsync(s.item_off.p, s.h_item_off.data(), (size_t(P) + 1) * 4, cudaMemcpyHostToDevice, st));
     TM_CUDA(cudaMemcpyAsync(s.chunk_off.p, s.h_chunk_off.data(), (size_t(P) + 1) * 4, cudaMemcpyHostToDevice, st));
-    s.slices.reserve(size_t(std::max<uint32_t>(chunks, 1)) * kBits * 8);
+    s.slices.reserve(size_t(std::max<uint32_t>(chunks, 1)) * kSliceWords);
     if (chunks) {
         k_slices<<<chunks, kChunk, 0, st>>>(s.queue.p, s.part_off.p, s.part_count.p, s.chunk_off.p, P, s.slices.p);
         TM_CHECK_LAUNCH();

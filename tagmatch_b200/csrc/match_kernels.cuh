@@ -69,6 +69,8 @@ __global__ void __launch_bounds__(kRouteThreads) k_route(const uint32_t *__restr
     }
 }
 
+constexpr int kSliceRows = kBits + 1;  // 192 bit rows + the all-zero padding row
+
 // Bit-sliced query masks of one 256-query chunk: z[b * 8 + w] bit l is set
 // when query 32 w + l of the chunk lacks filter bit b, or does not exist
 // (so an absent query is never a candidate).
@@ -102,9 +104,10 @@ __global__ void __launch_bounds__(kChunk) k_slices(const uint32_t *__restrict__ 
             if (lane == (unsigned)b) mine[k] = z;
         }
     }
-    uint32_t *zc = slices + size_t(c) * kBits * 8;
+    uint32_t *zc = slices + size_t(c) * kSliceRows * 8;
 #pragma unroll
     for (int k = 0; k < kWords; ++k) zc[(k * 32 + lane) * 8 + w] = mine[k];
+    if (lane == 0) zc[kNoBit * 8 + w] = 0u;  // the padding row: no query lacks it
 }
 
 // ---------------------------------------------------------------------------
@@ -159,7 +162,7 @@ struct MatchArgs {
     unsigned long long *work;
 };
 
-constexpr int kSliceWords = kBits * 8;  // 192 x 256 bits
+constexpr int kSliceWords = kSliceRows * 8;  // 193 x 256 bits
 
 // One staging buffer: a chunk's query records and slices.
 struct __align__(128) Stage {
@@ -239,6 +242,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
     __shared__ Stage st[2];
     __shared__ __align__(16) Pair s_out[kMatchWarps][kWarpBuf];
     __shared__ __align__(16) uint32_t s_list[kMatchWarps][kChunk + 4];  // per-warp candidate lists
+    __shared__ uint32_t s_nout[kMatchWarps];                             // pairs staged per warp
     __shared__ __align__(8) uint64_t full[2], empty[2];
     __shared__ uint32_t s_item[2];
     __shared__ int s_fail;
@@ -252,9 +256,9 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
+    if (tid < kMatchWarps) s_nout[tid] = 0;
     __syncthreads();
     if (tid == 0) produce(a, total, st, full, s_item, 0);
-    uint32_t nout = 0;  // staged pairs in this warp's buffer
     uint32_t w_tiles = 0, w_bits = 0, w_cand = 0, w_trips = 0, w_items = 0;
     for (uint32_t it = 0;; ++it) {
         const int b = it & 1;
@@ -283,19 +287,16 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
             const TileInfo ti = a.tile_info[t];
             const bool lane_valid = lane < ti.count;
             if (COUNT) ++w_tiles;
-            // candidates: queries holding every bit of the tile's AND mask;
-            // lane w < 8 builds the word for queries 32 w .. 32 w + 31
+            // candidates: queries holding the tile's selection bits; lane
+            // w < 8 ORs the "lacks" slices for queries 32 w .. 32 w + 31
             uint32_t lack = 0;
-#pragma unroll
-            for (int k = 0; k < kWords; ++k) {
-                uint32_t m = ti.and_mask[k];
-                while (m) {
-                    const uint32_t bit = k * 32 + __ffs(m) - 1;
-                    m &= m - 1;
-                    if (COUNT) ++w_bits;
-                    if (lane < 8) lack |= sz[bit * 8 + lane];
-                }
+            if (lane < 8) {
+                const uint32_t *zl = sz + lane;
+                lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
+                       zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] | zl[(ti.sel[1] & 0xFFu) * 8] |
+                       zl[((ti.sel[1] >> 8) & 0xFFu) * 8] | zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
             }
+            if (COUNT) w_bits += kSelBits;
             uint32_t cand_word = lane < 8 ? ~lack : 0u;
             if (lane < 8 && lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
             // compact candidate list (uint4 index of each query record):
@@ -353,34 +354,45 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
                 const bool h1 = lane_valid && x1 == 0 && i + 1 < n;
                 const bool h2 = lane_valid && x2 == 0 && i + 2 < n;
                 const bool h3 = lane_valid && x3 == 0 && i + 3 < n;
-                if (__any_sync(kFull, h0 | h1 | h2 | h3)) {
-                    const uint32_t m0 = __ballot_sync(kFull, h0), m1 = __ballot_sync(kFull, h1);
-                    const uint32_t m2 = __ballot_sync(kFull, h2), m3 = __ballot_sync(kFull, h3);
-                    const uint32_t nh = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
-                    if (nout + nh > (uint32_t)kWarpBuf) {
-                        flush_warp(s_out[warp], nout, a, lane);
-                        nout = 0;
-                    }
-                    const uint32_t below = (1u << lane) - 1u;
+                const uint32_t hb = uint32_t(h0) | (uint32_t(h1) << 1) | (uint32_t(h2) << 2) | (uint32_t(h3) << 3);
+                if (hb) {
+                    // usually one lane with one hit: a shared-memory atomic
+                    // reserves its slots; slots past the buffer go to global
+                    const uint32_t c = __popc(hb);
+                    uint32_t pos = atomicAdd(&s_nout[warp], c);
                     const uint32_t slot = t * kTile + lane;
-                    uint32_t base = nout;
-                    if (h0) s_out[warp][base + __popc(m0 & below)] = Pair{p1.z, slot};
-                    base += __popc(m0);
-                    if (h1) s_out[warp][base + __popc(m1 & below)] = Pair{q1.z, slot};
-                    base += __popc(m1);
-                    if (h2) s_out[warp][base + __popc(m2 & below)] = Pair{r1.z, slot};
-                    base += __popc(m2);
-                    if (h3) s_out[warp][base + __popc(m3 & below)] = Pair{u1.z, slot};
-                    nout += nh;
-                    __syncwarp();
+                    const uint32_t qid[4] = {p1.z, q1.z, r1.z, u1.z};
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        if ((hb >> k) & 1u) {
+                            const Pair pr{qid[k], slot};
+                            if (pos < (uint32_t)kWarpBuf) {
+                                s_out[warp][pos] = pr;
+                            } else {
+                                const unsigned long long g = atomicAdd(&a.counters[1], 1ull);
+                                if (g < a.pair_cap) a.pairs[g] = pr;
+                            }
+                            ++pos;
+                        }
+                    }
                 }
+            }
+            __syncwarp();
+            // flush the warp's buffer when it is more than half full
+            const uint32_t held = s_nout[warp];
+            if (held >= (uint32_t)kWarpBuf / 2) {
+                flush_warp(s_out[warp], min(held, (uint32_t)kWarpBuf), a, lane);
+                if (lane == 0) s_nout[warp] = 0;
+                __syncwarp();
             }
             __syncwarp();  // the list is rebuilt for the next tile
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[b]);
     }
-    if (nout) flush_warp(s_out[warp], nout, a, lane);
+    __syncwarp();
+    const uint32_t held = s_nout[warp];
+    if (held) flush_warp(s_out[warp], min(held, (uint32_t)kWarpBuf), a, lane);
     if (COUNT && lane == 0) {
         atomicAdd(&a.work[0], (unsigned long long)w_tiles);
         atomicAdd(&a.work[1], (unsigned long long)w_bits);

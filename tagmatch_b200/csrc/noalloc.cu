@@ -175,7 +175,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     TM_CUDA(cudaStreamSynchronize(st));
 
     uint32_t *queue = ar.take<uint32_t>(size_t(std::max<uint32_t>(routed, 1)) * kQueueWords, "partition queues");
-    uint32_t *slices = ar.take<uint32_t>(size_t(std::max<uint32_t>(chunks, 1)) * kBits * 8, "query slices");
+    uint32_t *slices = ar.take<uint32_t>(size_t(std::max<uint32_t>(chunks, 1)) * kSliceWords, "query slices");
     for (uint32_t p0 = 0; p0 < P; p0 += kMaxRouteParts) {
         const uint32_t pw = std::min(kMaxRouteParts, P - p0);
         const size_t smem = size_t(pw) * (kWords + 2) * sizeof(uint32_t);

@@ -365,6 +365,7 @@ void gpu_partition(const uint32_t *d_filters, uint32_t n, uint32_t max_p, bool w
     if (max_p == 0) throw Error(TM_ERR_INVALID, "partition size must be at least 1");
     out.n = n;
     out.parts.clear();
+    out.bit_freq.assign(kBits, 0);
     out.words.reserve(size_t(n) * kWords);
     out.order.reserve(n);
     if (with_tiles) out.tile_mark.reserve(n);
@@ -421,7 +422,8 @@ void gpu_partition(const uint32_t *d_filters, uint32_t n, uint32_t max_p, bool w
             // bit frequencies of the whole table -> tile-split weights:
             // a query lacks bit b with estimated probability
             // (1 - freq_b / n)^kTileWeightExp
-            std::vector<uint32_t> rf(kBits);
+            std::vector<uint32_t> &rf = out.bit_freq;
+            rf.assign(kBits, 0);
             TM_CUDA(cudaMemcpyAsync(rf.data(), freq.p, kBits * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
             TM_CUDA(cudaStreamSynchronize(st));
             std::vector<float> w(kBits);
@@ -479,11 +481,14 @@ void gpu_partition(const uint32_t *d_filters, uint32_t n, uint32_t max_p, bool w
 namespace {
 
 // One warp per tile: transposes the members into [6][32] words, ANDs them,
-// and records the original filter index of every lane.
+// records the original filter index of every lane, and picks the tile's
+// selection bits: the first kSelBits bits of the AND in `bit_order` (rarest
+// in the table first).
 __global__ void k_build_tiles(const uint32_t *__restrict__ words, const uint32_t *__restrict__ order,
                               const uint32_t *__restrict__ tile_begin /* n_tiles + 1 */, uint32_t n_tiles,
                               const uint32_t *__restrict__ part_tile_begin, uint32_t n_parts,
-                              uint32_t *__restrict__ tile_words, TileInfo *__restrict__ info,
+                              const uint8_t *__restrict__ bit_order, uint32_t *__restrict__ tile_words,
+                              TileInfo *__restrict__ info, uint32_t *__restrict__ tile_and,
                               uint32_t *__restrict__ slot_filter) {
     const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
@@ -500,19 +505,27 @@ __global__ void k_build_tiles(const uint32_t *__restrict__ words, const uint32_t
     uint32_t am[kWords];
 #pragma unroll
     for (int k = 0; k < kWords; ++k) am[k] = __reduce_and_sync(kFull, valid ? w[k] : 0xFFFFFFFFu);
+    if (lane < 8) tile_and[size_t(t) * 8 + lane] = lane < kWords ? am[lane < kWords ? lane : 0] : 0u;
     if (lane == 0) {
-        // owning partition: last p with part_tile_begin[p] <= t
-        uint32_t lo = 0, hi = n_parts;
+        uint32_t lo = 0, hi = n_parts;  // owning partition: last p with part_tile_begin[p] <= t
         while (hi - lo > 1) {
             uint32_t mid = (lo + hi) >> 1;
             if (part_tile_begin[mid] <= t) lo = mid;
             else hi = mid;
         }
-        // skip empty partitions that share the start
-        while (lo + 1 < n_parts && part_tile_begin[lo + 1] <= t) ++lo;
+        uint32_t sel[2] = {0, 0};
+        int k = 0;
+        for (int i = 0; i < kBits && k < kSelBits; ++i) {
+            const uint32_t bit = bit_order[i];
+            if ((am[bit >> 5] >> (bit & 31)) & 1u) {
+                sel[k >> 2] |= bit << (8 * (k & 3));
+                ++k;
+            }
+        }
+        for (; k < kSelBits; ++k) sel[k >> 2] |= kNoBit << (8 * (k & 3));
         TileInfo ti;
-#pragma unroll
-        for (int k = 0; k < kWords; ++k) ti.and_mask[k] = am[k];
+        ti.sel[0] = sel[0];
+        ti.sel[1] = sel[1];
         ti.count = cnt;
         ti.partition = lo;
         info[t] = ti;
@@ -533,8 +546,8 @@ __global__ void k_part_tiles(const Range *__restrict__ parts, uint32_t n_parts, 
     if (p == 0) part_tile_begin[n_parts] = n_parts ? mark_off[parts[n_parts - 1].end] : 0;
 }
 
-__global__ void k_part_mask(const TileInfo *__restrict__ info, const uint32_t *__restrict__ part_tile_begin, uint32_t n_parts,
-                            uint32_t *__restrict__ part_mask) {
+__global__ void k_part_mask(const uint32_t *__restrict__ tile_and, const uint32_t *__restrict__ part_tile_begin,
+                            uint32_t n_parts, uint32_t *__restrict__ part_mask) {
     const uint32_t p = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const unsigned lane = threadIdx.x & 31;
     if (p >= n_parts) return;
@@ -544,7 +557,7 @@ __global__ void k_part_mask(const TileInfo *__restrict__ info, const uint32_t *_
     for (int k = 0; k < kWords; ++k) m[k] = 0xFFFFFFFFu;
     for (uint32_t t = tb + lane; t < te; t += 32) {
 #pragma unroll
-        for (int k = 0; k < kWords; ++k) m[k] &= info[t].and_mask[k];
+        for (int k = 0; k < kWords; ++k) m[k] &= tile_and[size_t(t) * 8 + k];
     }
 #pragma unroll
     for (int k = 0; k < kWords; ++k) m[k] = __reduce_and_sync(kFull, m[k]);
@@ -587,7 +600,7 @@ __global__ void k_max_key(const uint32_t *__restrict__ keys, size_t n, uint32_t 
 }  // namespace
 
 size_t DevTable::device_bytes() const {
-    return tile_words.cap * sizeof(uint32_t) + tile_info.cap * sizeof(TileInfo) + part_tile_begin.cap * 4 +
+    return tile_words.cap * sizeof(uint32_t) + tile_info.cap * sizeof(TileInfo) + tile_and.cap * 4 + part_tile_begin.cap * 4 +
            part_mask.cap * 4 + slot_key_off.cap * 4 + keys.cap * 4 + slot_filter.cap * 4;
 }
 
@@ -626,16 +639,26 @@ void build_table(const PartitionResult &pr, const uint32_t *d_key_off, const uin
     TM_CHECK_LAUNCH();
     t.tile_words.reserve(n_slots * kWords);
     t.tile_info.reserve(nt);
+    t.tile_and.reserve(size_t(std::max<uint32_t>(nt, 1)) * 8);
     t.slot_filter.reserve(n_slots);
+    // selection bits are taken rarest-first over the whole table
+    std::vector<uint8_t> order_h(kBits);
+    for (int b = 0; b < kBits; ++b) order_h[b] = uint8_t(b);
+    std::stable_sort(order_h.begin(), order_h.end(),
+                     [&](uint8_t x, uint8_t y) { return pr.bit_freq[x] < pr.bit_freq[y]; });
+    DevBuf<uint8_t> bit_order;
+    bit_order.reserve(kBits);
+    TM_CUDA(cudaMemcpyAsync(bit_order.p, order_h.data(), kBits, cudaMemcpyHostToDevice, st));
     if (nt) {
         k_build_tiles<<<blocks_for(size_t(nt) * 32, 256), 256, 0, st>>>(pr.words.p, pr.order.p, tile_begin.p, nt,
-                                                                       t.part_tile_begin.p, t.n_parts, t.tile_words.p,
-                                                                       t.tile_info.p, t.slot_filter.p);
+                                                                       t.part_tile_begin.p, t.n_parts, bit_order.p,
+                                                                       t.tile_words.p, t.tile_info.p, t.tile_and.p,
+                                                                       t.slot_filter.p);
         TM_CHECK_LAUNCH();
     }
     t.part_mask.reserve(size_t(std::max<uint32_t>(t.n_parts, 1)) * 8);
     if (t.n_parts) {
-        k_part_mask<<<blocks_for(size_t(t.n_parts) * 32, 256), 256, 0, st>>>(t.tile_info.p, t.part_tile_begin.p, t.n_parts,
+        k_part_mask<<<blocks_for(size_t(t.n_parts) * 32, 256), 256, 0, st>>>(t.tile_and.p, t.part_tile_begin.p, t.n_parts,
                                                                             t.part_mask.p);
         TM_CHECK_LAUNCH();
     }

@@ -32,6 +32,7 @@ struct PartitionResult {
     DevBuf<uint32_t> words;          // [n][6] filters in partition order
     DevBuf<uint32_t> order;          // [n] original index of each position
     DevBuf<uint32_t> tile_mark;      // [n] 1 where a tile starts (with_tiles only)
+    std::vector<uint32_t> bit_freq;  // [192] bit frequencies over the whole table
 };
 
 // Device table used by the matcher.
@@ -41,6 +42,7 @@ struct DevTable {
     uint32_t max_key = 0;
     DevBuf<uint32_t> tile_words;      // [n_tiles][6][32]
     DevBuf<TileInfo> tile_info;       // [n_tiles]
+    DevBuf<uint32_t> tile_and;        // [n_tiles][8]: AND of the members (6 words), pad
     DevBuf<uint32_t> part_tile_begin; // [n_parts + 1]
     DevBuf<uint32_t> part_mask;       // [n_parts][8]: 6 mask words, tile count, pad
     DevBuf<uint32_t> slot_key_off;    // [n_tiles * 32 + 1]

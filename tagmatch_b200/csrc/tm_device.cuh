@@ -17,10 +17,14 @@ constexpr int kChunk = 256;        // queries per partition batch (QUERIES_BATCH
 constexpr int kQueueWords = 8;     // queued query record: 6 filter words, query id, pad (32 bytes)
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
-// Tile descriptor: AND of the tile's filters (the bits every member has),
-// member count and owning partition; 32 bytes.
+// Tile descriptor (16 bytes): the positions of up to 8 bits that every
+// member of the tile holds, most selective (rarest in the table) first,
+// padded with kNoBit; member count; owning partition.  A query lacking any
+// of these bits matches no filter of the tile.
+constexpr int kSelBits = 8;
+constexpr uint32_t kNoBit = 192;  // selects the all-zero slice row
 struct __align__(16) TileInfo {
-    uint32_t and_mask[kWords];
+    uint32_t sel[2];  // 8 bit positions, one per byte
     uint32_t count;
     uint32_t partition;
 };
