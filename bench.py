@@ -263,13 +263,11 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kern_s / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "k_match_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "k_match_traffic.txt")
     if os.path.exists(prof):
-        with open(prof) as fh:
-            pj = json.load(fh)
-        # scale the captured small case to a full launch by dense work
-        if pj.get("dense_tests_per_launch"):
-            traffic = pj["dram_bytes_per_launch"] * (st["dense_tests"] / launches) / pj["dense_tests_per_launch"]
+        kv = dict(l.strip().split("=", 1) for l in open(prof) if "=" in l and not l.startswith("#"))
+        # the captured case is smaller than a full launch; scale by queries
+        traffic = round(float(kv["dram_bytes"]) * (st["queries"] / launches) / float(kv["queries_per_launch"]))
     int_ops = 6 * st["dense_tests"] / launches
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
