@@ -350,11 +350,10 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
                 x1 = andnot_or(f[5], q1.y, x1);
                 x2 = andnot_or(f[5], r1.y, x2);
                 x3 = andnot_or(f[5], u1.y, x3);
-                const bool h0 = lane_valid && x0 == 0;
-                const bool h1 = lane_valid && x1 == 0 && i + 1 < n;
-                const bool h2 = lane_valid && x2 == 0 && i + 2 < n;
-                const bool h3 = lane_valid && x3 == 0 && i + 3 < n;
-                const uint32_t hb = uint32_t(h0) | (uint32_t(h1) << 1) | (uint32_t(h2) << 2) | (uint32_t(h3) << 3);
+                // common case: no hit among the four (one min chain)
+                if (min(min(x0, x1), min(x2, x3)) != 0 || !lane_valid) continue;
+                const uint32_t hb = uint32_t(x0 == 0) | (uint32_t(x1 == 0 && i + 1 < n) << 1) |
+                                    (uint32_t(x2 == 0 && i + 2 < n) << 2) | (uint32_t(x3 == 0 && i + 3 < n) << 3);
                 if (hb) {
                     // usually one lane with one hit: a shared-memory atomic
                     // reserves its slots; slots past the buffer go to global
