@@ -329,3 +329,27 @@ def test_serve_bench_runs():
     assert {l["mode"] for l in lines} == {"plain", "continuous"}
     for l in lines:
         assert l["requests"] > 0 and l["p99_ms"] >= l["p50_ms"] > 0
+
+
+@pytest.mark.skipif(not os.environ.get("TM_SCALE_TEST"), reason="set TM_SCALE_TEST=1: 100M-filter table (minutes)")
+def test_config2_scale_sampled_parity():
+    """100,000,000 filters (Zipf s=1.3, seed 3): the GPU partitioner and
+    table build at full size; sampled queries at superset fractions 10%, 50%
+    and 90% against the oracle; match_unique equals the sorted unique match
+    output; partitions respect the 65,536 maximum."""
+    n = int(os.environ.get("TM_SCALE_FILTERS", "100000000"))
+    f, ko, k = workload.generate_filters(n, 3, zipf_s=1.3)
+    tm = engine_with(f, ko, k, 65536)
+    info = tm.table_info()
+    assert info["filters"] == n and info["partitions"] >= n // 65536
+    for sup in (0.1, 0.5, 0.9):
+        q = workload.generate_queries(4096, f, 3, zipf_s=1.3, superset_fraction=sup)
+        off, keys = tm.match_batch(q)
+        uoff, ukeys = tm.match_batch(q, unique=True)
+        sample = np.arange(0, 4096, 256)
+        so, sk = oracle.match(f, ko, k, q[sample])
+        for j, i in enumerate(sample):
+            assert np.array_equal(np.sort(keys[off[i]:off[i + 1]]), np.sort(sk[so[j]:so[j + 1]]))
+        for i in range(0, 4096, 61):
+            assert np.array_equal(np.unique(keys[off[i]:off[i + 1]]), ukeys[uoff[i]:uoff[i + 1]])
+    tm.close()
