@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--queries", type=int, default=QUERIES)
     ap.add_argument("--batch", type=int, default=131072, help="queries per device batch")
     ap.add_argument("--unique", action="store_true", help="time match_unique instead of match")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -225,6 +226,12 @@ def run_ours(args):
     base = dq.data_ptr()
     nq = q.shape[0]
     B = args.batch
+    tuned = None
+    if not args.no_autotune:
+        # tiles per work item and device batch size, timed on a sample
+        seg, bl, tqps = tm.autotune(q[: min(nq, 262144)])
+        B = bl
+        tuned = {"seg_tiles": seg, "device_batch": bl, "sample_queries_per_s": round(tqps, 1)}
 
     def step():
         keys = 0
@@ -284,6 +291,7 @@ def run_ours(args):
                                    f"partitions <= {MAX_P}, 256-query partition batches, "
                                    f"{'match_unique' if args.unique else 'match'}",
                        "filters": args.filters, "queries_per_step_per_gpu": nq, "device_batch": B,
+                       "autotuned": tuned,
                        "partitions": info["partitions"], "tiles": info["tiles"],
                        "table_device_bytes": info["device_bytes"],
                        "l2": "inputs larger than L2 (table %.0f MB + per-step queues and results)" % (

@@ -8,6 +8,7 @@ Outputs (next to this file):
   libtm_workload.so     seeded workload generator (CPU)
   tagmatch_facade_test  C++ facade test driver (tagmatch.hh-compatible API)
   tagmatch_serve_bench  serving load generator over the C ABI (tm_submit)
+  tagmatch_driver       streaming driver (tagmatch_main.cc flow) and partition file writer
 """
 import os
 import subprocess
@@ -29,6 +30,7 @@ LIB = os.path.join(HERE, "libtagmatch_b200.so")
 WORKLOAD_LIB = os.path.join(HERE, "libtm_workload.so")
 FACADE_TEST = os.path.join(HERE, "tagmatch_facade_test")
 SERVE_BENCH = os.path.join(HERE, "tagmatch_serve_bench")
+DRIVER = os.path.join(HERE, "tagmatch_driver")
 
 
 def _run(cmd):
@@ -83,6 +85,15 @@ def build_serve_bench(quick=False):
     return SERVE_BENCH
 
 
+def build_driver(quick=False):
+    src = os.path.join(CSRC, "tagmatch_driver.cc")
+    if quick and not _stale(DRIVER, [src, LIB]):
+        return DRIVER
+    _run([CXX, "-O2", "-std=c++17", "-I" + os.path.join(INCLUDE, "tagmatch"), "-I" + INCLUDE, "-o", DRIVER, src,
+          "-L" + HERE, "-ltagmatch_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"])
+    return DRIVER
+
+
 def build_oracle():
     _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
 
@@ -92,6 +103,7 @@ def build_all(quick=False):
     build_engine(quick)
     build_facade_test(quick)
     build_serve_bench(quick)
+    build_driver(quick)
 
 
 if __name__ == "__main__":

@@ -217,6 +217,12 @@ int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p
     }
 }
 
+int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch_limit,
+                double *queries_per_s) {
+    if (!e || !queries || n == 0 || !seg_tiles || !batch_limit || !queries_per_s) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.autotune(queries, n, seg_tiles, batch_limit, queries_per_s); });
+}
+
 int tm_get_table_info(tm_engine *e, tm_table_info *info) {
     if (!e || !info) return TM_ERR_INVALID;
     return guard(e, [&] {

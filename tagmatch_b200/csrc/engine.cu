@@ -474,6 +474,69 @@ void Engine::match_device_noalloc(const uint32_t *d_queries, uint32_t nq, bool u
     match_batch_noalloc(d.table, d_queries, nq, unique, d_offsets, d_keys, capacity, n_keys, st ? st : d.stream);
 }
 
+void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, uint32_t *batch_out, double *qps_out) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (!already_consolidated_) throw Error(TM_ERR_STATE, "autotune before consolidate()");
+    if (n == 0) throw Error(TM_ERR_INVALID, "autotune needs a sample of queries");
+    Device &d = device(0);
+    if (dev_version_[0] != table_version_) build_device_table(d);
+    TM_CUDA(cudaSetDevice(d.id));
+    DevBuf<uint32_t> dq;
+    dq.reserve(size_t(n) * kWords);
+    TM_CUDA(cudaMemcpyAsync(dq.p, queries, size_t(n) * 24, cudaMemcpyHostToDevice, d.stream));
+    cudaEvent_t e0, e1;
+    TM_CUDA(cudaEventCreate(&e0));
+    TM_CUDA(cudaEventCreate(&e1));
+    double best = -1.0;
+    uint32_t best_seg = seg_tiles_, best_batch = batch_limit_;
+    const uint32_t segs[] = {32, 64, 128, 256, 512};
+    const uint32_t batches[] = {8192, 16384, 32768, 65536, 131072, 262144};
+    try {
+        for (uint32_t b : batches) {
+            if (b > n && b != batches[0]) break;
+            const uint32_t bb = std::min(b, n);
+            for (uint32_t sg : segs) {
+                d.scratch.seg_tiles = sg;
+                const uint64_t *doff;
+                const uint32_t *dkeys;
+                uint64_t nk;
+                BatchStats bs;
+                // one untimed pass (buffers grow), then the timed pass over the sample
+                match_batch(d.table, dq.p, bb, false, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
+                TM_CUDA(cudaEventRecord(e0, d.stream));
+                for (uint32_t q0 = 0; q0 + bb <= n; q0 += bb)
+                    match_batch(d.table, dq.p + size_t(q0) * kWords, bb, false, d.scratch, &doff, &dkeys, &nk, &bs, d.stream);
+                TM_CUDA(cudaEventRecord(e1, d.stream));
+                TM_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                TM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                const double qps = double(n / bb * bb) / (ms / 1e3);
+                if (qps > best) {
+                    best = qps;
+                    best_seg = sg;
+                    best_batch = bb;
+                }
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        d.scratch.seg_tiles = seg_tiles_;
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    seg_tiles_ = best_seg;
+    batch_limit_ = best_batch;
+    for (auto &dv : devs_) {
+        dv->scratch.seg_tiles = dv->scratch2.seg_tiles = best_seg;
+        for (auto &ln : dv->lanes) ln.scratch.seg_tiles = best_seg;
+    }
+    *seg_out = best_seg;
+    *batch_out = best_batch;
+    *qps_out = best;
+}
+
 void Engine::set_profiling(bool on) {
     std::lock_guard<std::mutex> lk(api_mtx_);
     profile_ = on;

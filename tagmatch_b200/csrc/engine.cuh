@@ -161,6 +161,10 @@ public:
     const EngineStats &stats() const { return stats_; }
     void reset_stats() { stats_ = EngineStats(); }
     void set_profiling(bool on);
+    // times the candidate tile segments per work item and device batch
+    // sizes on a sample of queries (device timing, CUDA events) and keeps
+    // the fastest; returns the chosen pair and its queries/s
+    void autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch, double *qps);
     bool profiling() const { return profile_; }
     bool started() const { return started_; }
     // host copy of the consolidated filters (table order) and keys
@@ -220,6 +224,7 @@ private:
     std::mutex api_mtx_;  // serialises synchronous calls
     EngineStats stats_;
     bool profile_ = false;
+    uint32_t seg_tiles_ = kSegTiles;
 
     // async path
     std::mutex q_mtx_;

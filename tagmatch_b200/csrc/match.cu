@@ -67,6 +67,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     for (int i = 0; i < 2 * ScanScratch::kLevels; ++i) scr.levels[i] = std::move(o.scr.levels[i]);
     sm_count = o.sm_count;
     pair_cap_hint = o.pair_cap_hint;
+    seg_tiles = o.seg_tiles;
     profile = o.profile;
     if (ev_begin) cudaEventDestroy(ev_begin);
     if (ev_end) cudaEventDestroy(ev_end);
@@ -157,7 +158,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         const uint32_t nc = (s.h_part_count[p] + kChunk - 1) / kChunk;
         const uint32_t nt = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
         chunks += nc;
-        items += nc * ((nt + kSegTiles - 1) / kSegTiles);
+        items += nc * ((nt + s.seg_tiles - 1) / s.seg_tiles);
     }
     s.h_chunk_off[P] = chunks;
     s.h_item_off[P] = items;
@@ -183,8 +184,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             TM_CUDA(cudaMemsetAsync(s.work.p, 0, 8 * sizeof(unsigned long long), st));
         }
         MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, s.part_count.p, s.part_off.p, s.item_off.p,
-                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.counters.p, s.pairs.p, (unsigned long long)s.pairs.cap,
-                    work_counters ? s.work.p : nullptr};
+                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p, s.pairs.p,
+                    (unsigned long long)s.pairs.cap, work_counters ? s.work.p : nullptr};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
             if (!s.ev_begin) {

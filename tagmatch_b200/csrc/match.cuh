@@ -6,7 +6,7 @@
 
 namespace tmb {
 
-constexpr int kSegTiles = 128;  // tiles per work item
+constexpr int kSegTiles = 128;  // default tiles per work item (tm_autotune may change it)
 
 // Device scratch for one in-flight batch (grow-only).
 struct MatchScratch {
@@ -33,6 +33,7 @@ struct MatchScratch {
     ScanScratch scr;
     int sm_count = 0;
     size_t pair_cap_hint = 0;
+    uint32_t seg_tiles = kSegTiles;  // tiles per work item
     // optional CUDA-event timing of the subset-test kernel
     bool profile = false;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;

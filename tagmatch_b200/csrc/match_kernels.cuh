@@ -153,6 +153,7 @@ struct MatchArgs {
     const uint32_t *queue;
     const uint32_t *slices;
     uint32_t n_parts;
+    uint32_t seg_tiles;            // tiles per work item
     unsigned long long *counters;  // [0] next item, [1] pairs, [2] error flags
     Pair *pairs;
     unsigned long long pair_cap;
@@ -212,8 +213,8 @@ __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
     const uint32_t chunk = local % nchunks, seg = local / nchunks;
     r.qbase = a.part_off[lo] + chunk * kChunk;
     r.nq = min((uint32_t)kChunk, pq - chunk * kChunk);
-    r.tb = a.part_tile_begin[lo] + seg * kSegTiles;
-    r.te = min(r.tb + (uint32_t)kSegTiles, a.part_tile_begin[lo + 1]);
+    r.tb = a.part_tile_begin[lo] + seg * a.seg_tiles;
+    r.te = min(r.tb + a.seg_tiles, a.part_tile_begin[lo + 1]);
     r.zchunk = a.chunk_off[lo] + chunk;
     return r;
 }

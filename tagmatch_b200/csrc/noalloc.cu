@@ -193,7 +193,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     if (pair_room < 256) throw Error(TM_ERR_CAPACITY, "no-allocation scratch exhausted before the pair buffer; split the batch");
     Pair *pairs = ar.take<Pair>(pair_room - 32, "matching pairs");
     MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, part_count, part_off, item_off, chunk_off, queue, slices,
-                P, counters, pairs, (unsigned long long)(pair_room - 32), nullptr};
+                P, uint32_t(kSegTiles), counters, pairs, (unsigned long long)(pair_room - 32), nullptr};
     k_match<false><<<unsigned(sms) * 4, kMatchThreads, 0, st>>>(a);
     TM_CHECK_LAUNCH();
     unsigned long long hc[3] = {0, 0, 0};

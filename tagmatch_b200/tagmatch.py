@@ -237,6 +237,16 @@ class TagMatch:
         self._check(self._lib.tm_get_table_info(self._h, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in info._fields_}
 
+    def autotune(self, sample_queries):
+        """Picks tiles per work item and the device batch size on a sample
+        (device timing); returns (seg_tiles, batch_limit, queries_per_s)."""
+        q = as_filters(sample_queries)
+        seg, bl = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        qps = ctypes.c_double(0)
+        self._check(self._lib.tm_autotune(self._h, _p32(q), q.shape[0], ctypes.byref(seg), ctypes.byref(bl),
+                                          ctypes.byref(qps)))
+        return seg.value, bl.value, qps.value
+
     def set_profiling(self, on):
         self._check(self._lib.tm_set_profiling(self._h, 1 if on else 0))
 

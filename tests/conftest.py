@@ -14,7 +14,7 @@ def pytest_configure(config):
 
 def _built():
     from tagmatch_b200 import build
-    return all(os.path.exists(p) for p in (build.LIB, build.WORKLOAD_LIB, build.FACADE_TEST, build.SERVE_BENCH))
+    return all(os.path.exists(p) for p in (build.LIB, build.WORKLOAD_LIB, build.FACADE_TEST, build.SERVE_BENCH, build.DRIVER))
 
 
 @pytest.fixture(scope="session", autouse=True)

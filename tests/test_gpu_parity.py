@@ -353,3 +353,88 @@ def test_config2_scale_sampled_parity():
         for i in range(0, 4096, 61):
             assert np.array_equal(np.unique(keys[off[i]:off[i + 1]]), ukeys[uoff[i]:uoff[i + 1]])
     tm.close()
+
+
+def _write_fib_entries(path, f, ko, k):
+    """fib_entry binary records: 24-byte filter, u32 n, n keys (fib.cc:14-21)."""
+    import struct
+    with open(path, "wb") as out:
+        for i in range(f.shape[0]):
+            b, e = int(ko[i]), int(ko[i + 1])
+            out.write(f[i].astype("<u4").tobytes())
+            out.write(struct.pack("<I", e - b))
+            out.write(np.asarray(k[b:e], dtype="<u4").tobytes())
+
+
+def test_streaming_driver_and_partition_files(tmp_path):
+    """tagmatch_main.cc's flow through the C++ facade (chunked loads,
+    consolidate, asynchronous match, stop drain) and the partitioning
+    client's output files (partition_prefix + partition_fib_entry)."""
+    import struct
+    f, ko, k = workload.generate_filters(20000, 47)
+    q = workload.generate_queries(2000, f, 47)
+    fp, qp = tmp_path / "filters.bin", tmp_path / "queries.bin"
+    _write_fib_entries(fp, f, ko, k)
+    q.astype("<u4").tofile(qp)
+    for unique in (0, 1):
+        out = subprocess.run([build.DRIVER, f"in={fp}", f"Q={qp}", "m=4096", f"unique={unique}",
+                              f"db={tmp_path / 'drv.db'}"], capture_output=True, text=True, timeout=600)
+        assert out.returncode == 0, out.stderr[-2000:]
+        line = [l for l in out.stdout.splitlines() if l.startswith("round=0")][0]
+        fields = dict(x.split("=") for x in line.split())
+        ooff, okeys = oracle.match(f, ko, k, q, unique=bool(unique))
+        assert int(fields["completed"]) == q.shape[0]
+        assert int(fields["keys"]) == okeys.size
+    # chunked: two rounds of 10,000 filters each, each matched on its own
+    out = subprocess.run([build.DRIVER, f"in={fp}", f"Q={qp}", "m=4096", "chunk=10000", f"db={tmp_path / 'drv.db'}"],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    rounds = [dict(x.split("=") for x in l.split()) for l in out.stdout.splitlines() if l.startswith("round=")]
+    assert len(rounds) == 2
+    for r, (a, b) in zip(rounds, [(0, 10000), (10000, 20000)]):
+        sub_ko = (ko[a:b + 1] - ko[a]).astype(np.uint32)
+        _, okeys = oracle.match(f[a:b], sub_ko, k[ko[a]:ko[b]], q)
+        assert int(r["keys"]) == okeys.size
+    # partition files of the reference partitioner's own seeded case
+    case = load_partitions_golden()["random"][0]
+    pf, pk, pkeys = workload.generate_filters(case["n"], case["seed"])
+    fp2 = tmp_path / "pfilters.bin"
+    _write_fib_entries(fp2, pf, pk, pkeys)
+    out = subprocess.run([build.DRIVER, f"in={fp2}", f"m={case['max_p']}", f"part_out={tmp_path / 'out'}",
+                          f"db={tmp_path / 'drv.db'}"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    raw = (tmp_path / "out.partitions").read_bytes()
+    rec = 24 + 1 + 4 + 4
+    assert len(raw) % rec == 0
+    parts = []
+    for i in range(len(raw) // rec):
+        r = raw[i * rec:(i + 1) * rec]
+        mask = np.frombuffer(r[:24], dtype="<u4")
+        length, pid, size = r[24], struct.unpack("<I", r[25:29])[0], struct.unpack("<I", r[29:33])[0]
+        assert length == 192 and pid == i
+        parts.append((mask, size))
+    fr = (tmp_path / "out.filters").read_bytes()
+    part_of, pos = [], 0
+    while pos < len(fr):
+        pid = struct.unpack("<I", fr[pos:pos + 4])[0]
+        filt = np.frombuffer(fr[pos + 4:pos + 28], dtype="<u4")
+        n = struct.unpack("<I", fr[pos + 28:pos + 32])[0]
+        assert oracle.subset_of(parts[pid][0], filt)
+        part_of.append(pid)
+        pos += 32 + 4 * n
+    assert groups_from_assignment(part_of, len(parts)) == groups_from_assignment(case["partition_of"],
+                                                                                 len(case["sizes"]))
+
+
+def test_autotune_keeps_results():
+    """tm_autotune picks tiles per work item and the batch size by timing;
+    matches are the same whatever it picks."""
+    f, ko, k = workload.generate_filters(100000, 48)
+    q = workload.generate_queries(20000, f, 48)
+    tm = engine_with(f, ko, k, 8192)
+    off0, keys0 = tm.match_batch(q)
+    seg, batch, qps = tm.autotune(q)
+    assert seg in (32, 64, 128, 256, 512) and batch in (8192, 16384, 20000) and qps > 0
+    off1, keys1 = tm.match_batch(q)
+    assert_same_multisets(off0, keys0, off1, keys1)
+    tm.close()
