@@ -438,3 +438,28 @@ def test_autotune_keeps_results():
     off1, keys1 = tm.match_batch(q)
     assert_same_multisets(off0, keys0, off1, keys1)
     tm.close()
+
+
+def test_latency_limit_flushes_without_stop():
+    """With a latency limit, a lone pending query completes without stop()
+    (front_end.cc:563-598: queues older than the limit are flushed); with no
+    limit it waits for a full batch or stop()."""
+    import time
+    f, ko, k = workload.generate_filters(5000, 49)
+    q = workload.generate_queries(10, f, 49)
+    tm = engine_with(f, ko, k, 1000)
+    done = threading.Event()
+    tm.set_latency_limit_ms(20)
+    tm.start(2, 1)
+    tm.match(q[0], lambda keys: done.set())
+    assert done.wait(10.0), "latency limit did not flush the pending query"
+    tm.stop()
+    tm.set_latency_limit_ms(0)
+    late = threading.Event()
+    tm.start(2, 1)
+    tm.match(q[1], lambda keys: late.set())
+    time.sleep(0.3)
+    assert not late.is_set()  # no limit: waits for a full batch or stop()
+    tm.stop()
+    assert late.is_set()
+    tm.close()
