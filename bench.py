@@ -313,8 +313,11 @@ def run_ours(args):
         except Exception:
             avail = None
         e2e_nq = nq
-        if avail is not None and need * 4 > 0.6 * avail:
-            e2e_nq = max(B, int(nq * 0.6 * avail / (need * 4)))
+        # the ranks of this node share its memory
+        local_ranks = int(os.environ.get("LOCAL_WORLD_SIZE", str(world)))
+        budget = 0.6 * avail / max(local_ranks, 1) if avail is not None else None
+        if budget is not None and need * 4 > budget:
+            e2e_nq = max(min(B, nq), int(nq * budget / (need * 4)))
             need = int(need * e2e_nq / nq) + 1024
         # caller-owned pinned output (the result keys of a whole step)
         out_keys = torch.empty(need, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)

@@ -47,8 +47,10 @@ typedef struct tm_engine tm_engine;
  * thread.  keys is valid only during the call. */
 typedef void (*tm_match_callback)(void *user, uint64_t tag, const uint32_t *keys, uint64_t n_keys);
 
-/* Creates / destroys an engine (the reference's static state).  Device
- * work starts at the first consolidate on CUDA device 0. */
+/* Creates / destroys an engine (the reference's static state).  The
+ * engine's first device is the calling thread's current CUDA device at
+ * tm_create (one process per GPU: set the device first); device work
+ * starts at the first consolidate. */
 int tm_create(tm_engine **out);
 void tm_destroy(tm_engine *e);
 const char *tm_last_error(const tm_engine *e);

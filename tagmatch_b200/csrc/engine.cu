@@ -23,7 +23,15 @@ void KeysetChange::apply(std::vector<uint32_t> &keys) const {
     keys.swap(out);
 }
 
-Engine::Engine() {}
+// Device i of the engine is CUDA device base_device_ + i, base_device_
+// being the calling thread's current device when the engine is created
+// (one process per GPU: each sets its device first).
+Engine::Engine() {
+    if (cudaGetDevice(&base_device_) != cudaSuccess) {
+        cudaGetLastError();
+        base_device_ = 0;
+    }
+}
 
 Engine::~Engine() {
     try {
@@ -164,7 +172,7 @@ void Engine::consolidate(uint32_t psize, uint32_t threads) {
 Engine::Device &Engine::device(int i) {
     while ((int)devs_.size() <= i) {
         auto d = std::make_unique<Device>();
-        d->id = int(devs_.size());
+        d->id = base_device_ + int(devs_.size());
         TM_CUDA(cudaSetDevice(d->id));
         TM_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
         devs_.push_back(std::move(d));
@@ -206,8 +214,9 @@ void Engine::start(uint32_t threads, uint32_t gpus) {
     if (gpus == 0) gpus = 1;
     int count = 0;
     TM_CUDA(cudaGetDeviceCount(&count));
-    if ((int)gpus > count) throw Error(TM_ERR_INVALID, "start(): " + std::to_string(gpus) + " GPUs requested, " +
-                                                            std::to_string(count) + " present");
+    if (base_device_ + (int)gpus > count)
+        throw Error(TM_ERR_INVALID, "start(): " + std::to_string(gpus) + " GPUs requested from device " +
+                                        std::to_string(base_device_) + ", " + std::to_string(count) + " present");
     threads_ = threads;
     if (started_) return;  // re-entrant, like front_end::start (front_end.cc:671-691)
     gpus_ = gpus;

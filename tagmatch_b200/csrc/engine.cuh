@@ -224,6 +224,7 @@ private:
     std::mutex api_mtx_;  // serialises synchronous calls
     EngineStats stats_;
     bool profile_ = false;
+    int base_device_ = 0;
     uint32_t seg_tiles_ = kSegTiles;
 
     // async path
