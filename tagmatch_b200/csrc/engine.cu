@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
@@ -42,11 +43,14 @@ Engine::~Engine() {
         if (!d) continue;
         cudaSetDevice(d->id);
         if (d->stream) cudaStreamDestroy(d->stream);
-        if (d->stream2) cudaStreamDestroy(d->stream2);
         for (auto &ln : d->lanes)
             if (ln.stream) cudaStreamDestroy(ln.stream);
-        for (cudaEvent_t ev : d->lane_done)
-            if (ev) cudaEventDestroy(ev);
+        for (auto &h : d->host) {
+            if (h.stream) cudaStreamDestroy(h.stream);
+            if (h.staged) cudaEventDestroy(h.staged);
+            for (cudaEvent_t ev : h.trace_ev)
+                if (ev) cudaEventDestroy(ev);
+        }
     }
 }
 
@@ -172,7 +176,8 @@ void Engine::consolidate(uint32_t psize, uint32_t threads) {
 Engine::Device &Engine::device(int i) {
     while ((int)devs_.size() <= i) {
         auto d = std::make_unique<Device>();
-        d->id = base_device_ + int(devs_.size());
+        d->index = int(devs_.size());
+        d->id = base_device_ + d->index;
         TM_CUDA(cudaSetDevice(d->id));
         TM_CUDA(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
         devs_.push_back(std::move(d));
@@ -199,7 +204,7 @@ void Engine::build_device_table(Device &d) {
     build_table(pr, ko.p, k.p, keys_.size(), d.table, d.stream);
     TM_CUDA(cudaStreamSynchronize(d.stream));
     d.table_ready = true;
-    dev_version_[d.id] = table_version_;
+    dev_version_[d.index] = table_version_;
 }
 
 uint32_t Engine::n_partitions() const { return devs_.empty() ? 0 : devs_[0]->table.n_parts; }
@@ -270,7 +275,7 @@ void Engine::clear() {
         TM_CUDA(cudaSetDevice(d->id));
         d->table = DevTable();
         d->scratch = MatchScratch();
-        d->scratch2 = MatchScratch();
+        for (auto &h : d->host) h.scratch = MatchScratch();
         for (auto &ln : d->lanes) ln.scratch = MatchScratch();
         d->table_ready = false;
     }
@@ -538,7 +543,8 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     seg_tiles_ = best_seg;
     batch_limit_ = best_batch;
     for (auto &dv : devs_) {
-        dv->scratch.seg_tiles = dv->scratch2.seg_tiles = best_seg;
+        dv->scratch.seg_tiles = best_seg;
+        for (auto &h : dv->host) h.scratch.seg_tiles = best_seg;
         for (auto &ln : dv->lanes) ln.scratch.seg_tiles = best_seg;
     }
     *seg_out = best_seg;
@@ -620,14 +626,35 @@ void parallel_widen(uint32_t *dst, const uint16_t *src, uint64_t n) {
     for (auto &x : th) x.join();
 }
 
+// Share of a batch's keys that crosses PCIe as 32-bit values straight into
+// a pinned caller buffer when the keys could travel narrowed to 16 bits.
+// Narrowed keys halve the bytes on the link but cost host memory bandwidth
+// (a 2-byte DMA write, a 2-byte read and a 4-byte write per key by the copy
+// threads); direct keys cost 4 bytes on the link and one 4-byte DMA write.
+// Sending part of each batch direct keeps the link and host memory both
+// below the matcher's time per batch.  TM_DIRECT_FRACTION overrides it.
+constexpr double kDirectFraction = 0.1;
+// smallest batch of match_host's final, halving batches
+constexpr uint64_t kTailBatch = 4096;
+
+double direct_fraction() {
+    const char *s = std::getenv("TM_DIRECT_FRACTION");
+    if (!s || !*s) return kDirectFraction;
+    return std::min(1.0, std::max(0.0, std::atof(s)));
+}
+
 }  // namespace
 
-// Batches alternate between two lanes (scratch + stream + pinned staging):
-// while one batch's results travel to the host, the next batch is matched.
-// Keys go straight into a pinned caller buffer; a pageable one is filled
-// from pinned staging by copy threads.  When every key of the table is
-// below 65,536 the keys cross PCIe as 16-bit values and copy threads widen
-// them into the caller's buffer (half the bytes on the link).
+// Batches rotate over three lanes (scratch + stream + pinned staging): while
+// one batch is matched, the results of the two before it cross PCIe and are
+// widened, so the device never waits for the host copies of the batch it
+// last finished.  Keys go to the caller's buffer in one of three ways:
+// - every key of the table below 65,536: a share direct_fraction() of the
+//   batch's keys is copied as 32-bit values straight into a pinned caller
+//   buffer; the rest crosses as 16-bit values into pinned staging and copy
+//   threads widen them into the caller's buffer;
+// - otherwise, pinned caller buffer: one 32-bit copy straight into it;
+// - otherwise: a 32-bit copy into pinned staging, then copy threads.
 void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
                         uint64_t capacity, uint64_t *n_keys) {
     std::lock_guard<std::mutex> lk(api_mtx_);
@@ -635,41 +662,75 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     Device &d = device(0);
     if (dev_version_[0] != table_version_) build_device_table(d);
     TM_CUDA(cudaSetDevice(d.id));
-    if (!d.stream2) TM_CUDA(cudaStreamCreateWithFlags(&d.stream2, cudaStreamNonBlocking));
-    for (int l = 0; l < 2; ++l)
-        if (!d.lane_done[l]) TM_CUDA(cudaEventCreateWithFlags(&d.lane_done[l], cudaEventDisableTiming));
-    MatchScratch *scr[2] = {&d.scratch, &d.scratch2};
-    cudaStream_t str[2] = {d.stream, d.stream2};
-    HostBuf<uint64_t> *hoff[2] = {&d.h_offsets, &d.h_offsets2};
-    HostBuf<uint32_t> *hkeys[2] = {&d.h_keys, &d.h_keys2};
-    HostBuf<uint16_t> *hk16[2] = {&d.h_keys16, &d.h_keys16b};
+    // TM_HOST_TRACE: one stderr line per batch with the host wait, match,
+    // copy and widening times (diagnostics)
+    static const bool trace = std::getenv("TM_HOST_TRACE") != nullptr;
+    using TClock = std::chrono::steady_clock;
+    const TClock::time_point t_call = TClock::now();
+    auto ms_at = [&](TClock::time_point t) { return std::chrono::duration<double, std::milli>(t - t_call).count(); };
+    MatchScratch *scr[kHostLanes];
+    cudaStream_t str[kHostLanes];
+    for (int l = 0; l < kHostLanes; ++l) {
+        HostLane &h = d.host[l];
+        if (l && !h.stream) TM_CUDA(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+        if (!h.staged) TM_CUDA(cudaEventCreateWithFlags(&h.staged, cudaEventDisableTiming));
+        scr[l] = l ? &h.scratch : &d.scratch;
+        str[l] = l ? h.stream : d.stream;
+        scr[l]->seg_tiles = seg_tiles_;
+        if (trace)
+            for (cudaEvent_t &ev : h.trace_ev)
+                if (!ev) TM_CUDA(cudaEventCreate(&ev));
+    }
     const bool narrow = d.table.max_key < 65536u;
-    const bool direct = !narrow && out_keys != nullptr && is_pinned(out_keys);
+    const bool pinned_out = out_keys != nullptr && is_pinned(out_keys);
+    const double frac = pinned_out ? direct_fraction() : 0.0;
     struct Pending {
         bool active = false;
-        uint64_t q0 = 0, base = 0, nk = 0;
+        uint64_t q0 = 0, base = 0, nk = 0, nd = 0;
         uint32_t n = 0;
-        bool staged = false;
         std::thread copier;
-    } pend[2];
+        uint64_t batch = 0;
+        TClock::time_point t_begin, t_matched, t_widen0, t_widen1;
+    } pend[kHostLanes];
     uint64_t total = 0;
     bool overflow = false;
     out_offsets[0] = 0;
     auto finish = [&](int l) {
         Pending &p = pend[l];
         if (!p.active) return;
+        const TClock::time_point t_wait = TClock::now();
         if (p.copier.joinable()) p.copier.join();
         TM_CUDA(cudaStreamSynchronize(str[l]));
-        const uint64_t *o = hoff[l]->p;
+        if (trace) {
+            float m16 = 0.f, m32 = 0.f;
+            cudaEventElapsedTime(&m16, d.host[l].trace_ev[0], d.host[l].trace_ev[1]);
+            cudaEventElapsedTime(&m32, d.host[l].trace_ev[1], d.host[l].trace_ev[2]);
+            std::fprintf(stderr,
+                         "[tm host] batch %llu lane %d keys %llu direct %llu begin %.1f matched %.1f widen %.1f-%.1f "
+                         "narrow_copy_ms %.1f direct_copy_ms %.1f finish_wait_ms %.1f\n",
+                         (unsigned long long)p.batch, l, (unsigned long long)p.nk, (unsigned long long)p.nd,
+                         ms_at(p.t_begin), ms_at(p.t_matched), ms_at(p.t_widen0), ms_at(p.t_widen1), m16, m32,
+                         ms_at(TClock::now()) - ms_at(t_wait));
+        }
+        const uint64_t *o = d.host[l].h_offsets.p;
         for (uint32_t i = 1; i <= p.n; ++i) out_offsets[p.q0 + i] = o[i] + p.base;
         p.active = false;
     };
     try {
         uint64_t it = 0;
-        for (uint64_t q0 = 0; q0 < nq; q0 += batch_limit_, ++it) {
-            const int l = int(it & 1);
+        for (uint64_t q0 = 0, step = 0; q0 < nq; q0 += step, ++it) {
+            // full batches, then the last batch_limit_ queries in halving
+            // batches (down to kTailBatch): what is left to copy and widen
+            // after the last match is then a small batch's results
+            const uint64_t left = nq - q0;
+            step = left > batch_limit_ ? batch_limit_
+                   : left <= 2 * kTailBatch ? left
+                                            : std::max<uint64_t>(kTailBatch, left / 2);
+            const uint32_t n = uint32_t(step);
+            const int l = int(it % kHostLanes);
             finish(l);
-            const uint32_t n = uint32_t(std::min<uint64_t>(batch_limit_, nq - q0));
+            const TClock::time_point t_begin = TClock::now();
+            HostLane &h = d.host[l];
             MatchScratch &sc = *scr[l];
             sc.queries.reserve(size_t(n) * kWords);
             TM_CUDA(cudaMemcpyAsync(sc.queries.p, queries + q0 * kWords, size_t(n) * 24, cudaMemcpyHostToDevice, str[l]));
@@ -681,52 +742,72 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             match_batch(d.table, sc.queries.p, n, unique, sc, &doff, &dkeys, &nk, &bs, str[l]);
             stats_.add(bs, n, profile_);
             stats_.h2d_bytes += uint64_t(n) * 24;
-            stats_.d2h_bytes += (uint64_t(n) + 1) * 8 + nk * (narrow ? 2 : 4);
-            hoff[l]->reserve(size_t(n) + 1);
-            TM_CUDA(cudaMemcpyAsync(hoff[l]->p, doff, (size_t(n) + 1) * 8, cudaMemcpyDeviceToHost, str[l]));
+            h.h_offsets.reserve(size_t(n) + 1);
+            TM_CUDA(cudaMemcpyAsync(h.h_offsets.p, doff, (size_t(n) + 1) * 8, cudaMemcpyDeviceToHost, str[l]));
+            stats_.d2h_bytes += (uint64_t(n) + 1) * 8;
             Pending &p = pend[l];
             p.active = true;
             p.q0 = q0;
             p.n = n;
             p.base = total;
             p.nk = nk;
-            p.staged = false;
-            if (!overflow && total + nk <= capacity) {
-                if (nk && narrow) {
-                    const uint16_t *d16 = narrow_keys(dkeys, nk, sc, str[l]);
-                    hk16[l]->reserve(nk);
-                    TM_CUDA(cudaMemcpyAsync(hk16[l]->p, d16, nk * 2, cudaMemcpyDeviceToHost, str[l]));
-                    TM_CUDA(cudaEventRecord(d.lane_done[l], str[l]));
-                    p.staged = true;
-                    cudaEvent_t ev = d.lane_done[l];
-                    uint32_t *dst = out_keys + total;
-                    const uint16_t *src = hk16[l]->p;
-                    p.copier = std::thread([=] {
-                        if (cudaEventSynchronize(ev) == cudaSuccess) parallel_widen(dst, src, nk);
-                    });
-                } else if (nk && direct) {
-                    TM_CUDA(cudaMemcpyAsync(out_keys + total, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
-                } else if (nk) {
-                    hkeys[l]->reserve(nk);
-                    TM_CUDA(cudaMemcpyAsync(hkeys[l]->p, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
-                    TM_CUDA(cudaEventRecord(d.lane_done[l], str[l]));
-                    p.staged = true;
-                    cudaEvent_t ev = d.lane_done[l];
-                    uint32_t *dst = out_keys + total;
-                    const uint32_t *src = hkeys[l]->p;
+            p.nd = 0;
+            p.batch = it;
+            p.t_begin = t_begin;
+            p.t_matched = TClock::now();
+            p.t_widen0 = p.t_widen1 = p.t_matched;
+            if (trace)  // all three recorded; the narrow path records [1] and [2] again after its copies
+                for (cudaEvent_t ev : h.trace_ev) TM_CUDA(cudaEventRecord(ev, str[l]));
+            if (!overflow && total + nk <= capacity && nk) {
+                uint32_t *dst = out_keys + total;
+                if (narrow) {
+                    // keys [0, nd) direct, [nd, nk) narrowed; nd a multiple
+                    // of 4 keeps the narrowing kernel on 16-byte loads
+                    const uint64_t nd = std::min<uint64_t>(nk, uint64_t(double(nk) * frac) & ~uint64_t(3));
+                    const uint64_t nn = nk - nd;
+                    p.nd = nd;
+                    if (nn) {
+                        const uint16_t *d16 = narrow_keys(dkeys + nd, nn, sc, str[l]);
+                        h.h_keys16.reserve(nn);
+                        TM_CUDA(cudaMemcpyAsync(h.h_keys16.p, d16, nn * 2, cudaMemcpyDeviceToHost, str[l]));
+                        TM_CUDA(cudaEventRecord(h.staged, str[l]));
+                        cudaEvent_t ev = h.staged;
+                        const uint16_t *src = h.h_keys16.p;
+                        uint32_t *wdst = dst + nd;
+                        Pending *pp = &p;
+                        p.copier = std::thread([=] {
+                            if (cudaEventSynchronize(ev) != cudaSuccess) return;
+                            if (trace) pp->t_widen0 = TClock::now();
+                            parallel_widen(wdst, src, nn);
+                            if (trace) pp->t_widen1 = TClock::now();
+                        });
+                    }
+                    if (trace) TM_CUDA(cudaEventRecord(h.trace_ev[1], str[l]));
+                    if (nd) TM_CUDA(cudaMemcpyAsync(dst, dkeys, nd * 4, cudaMemcpyDeviceToHost, str[l]));
+                    if (trace) TM_CUDA(cudaEventRecord(h.trace_ev[2], str[l]));
+                    stats_.d2h_bytes += nn * 2 + nd * 4;
+                } else if (pinned_out) {
+                    TM_CUDA(cudaMemcpyAsync(dst, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
+                    stats_.d2h_bytes += nk * 4;
+                } else {
+                    h.h_keys.reserve(nk);
+                    TM_CUDA(cudaMemcpyAsync(h.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, str[l]));
+                    TM_CUDA(cudaEventRecord(h.staged, str[l]));
+                    cudaEvent_t ev = h.staged;
+                    const uint32_t *src = h.h_keys.p;
                     p.copier = std::thread([=] {
                         if (cudaEventSynchronize(ev) == cudaSuccess) parallel_copy(dst, src, nk * 4);
                     });
+                    stats_.d2h_bytes += nk * 4;
                 }
-            } else {
+            } else if (nk) {
                 overflow = true;
             }
             total += nk;
         }
-        finish(0);
-        finish(1);
+        for (int l = 0; l < kHostLanes; ++l) finish(l);
     } catch (...) {
-        for (int l = 0; l < 2; ++l)
+        for (int l = 0; l < kHostLanes; ++l)
             if (pend[l].copier.joinable()) pend[l].copier.join();
         throw;
     }

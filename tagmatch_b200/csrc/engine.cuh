@@ -186,18 +186,28 @@ private:
         RequestPtr r;
         uint32_t q0, n;
     };
+    // One stage of match_host's pipeline: device scratch, a stream, and the
+    // pinned staging its results cross PCIe into.  Lane 0 borrows the
+    // device's own scratch and stream (shared with match_device).
+    static constexpr int kHostLanes = 3;
+    struct HostLane {
+        MatchScratch scratch;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t staged = nullptr;
+        cudaEvent_t trace_ev[3] = {nullptr, nullptr, nullptr};  // TM_HOST_TRACE: matched, narrow copied, direct copied
+        HostBuf<uint64_t> h_offsets;
+        HostBuf<uint32_t> h_keys;
+        HostBuf<uint16_t> h_keys16;
+    };
     struct Device {
-        int id = 0;
-        cudaStream_t stream = nullptr, stream2 = nullptr;
-        cudaEvent_t lane_done[2] = {nullptr, nullptr};
+        int index = 0;  // position in devs_ (and dev_version_)
+        int id = 0;     // CUDA device: base_device_ + index
+        cudaStream_t stream = nullptr;
         DevTable table;
-        MatchScratch scratch, scratch2;  // two pipeline lanes of match_host
+        MatchScratch scratch;
         bool table_ready = false;
-        HostBuf<uint32_t> h_queries;
-        HostBuf<uint64_t> h_offsets, h_offsets2;
-        HostBuf<uint32_t> h_keys, h_keys2;
-        HostBuf<uint16_t> h_keys16, h_keys16b;
-        Lane lanes[kLanes];  // asynchronous matcher lanes
+        HostLane host[kHostLanes];  // synchronous host-buffer pipeline
+        Lane lanes[kLanes];         // asynchronous matcher lanes
     };
     void build_device_table(Device &d);
     Device &device(int i);

@@ -39,6 +39,7 @@
 // (the reference truncates silently at 4,194,304 hits, gpu.cu:55).
 #include "match_kernels.cuh"
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 
 namespace tmb {
@@ -64,6 +65,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     ucount = std::move(o.ucount);
     uoff = std::move(o.uoff);
     ukeys = std::move(o.ukeys);
+    readback = std::move(o.readback);
     for (int i = 0; i < 2 * ScanScratch::kLevels; ++i) scr.levels[i] = std::move(o.scr.levels[i]);
     sm_count = o.sm_count;
     pair_cap_hint = o.pair_cap_hint;
@@ -85,6 +87,21 @@ const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s,
         TM_CHECK_LAUNCH();
     }
     return s.keys16.p;
+}
+
+// Reads na words at a and nb words at b (device memory) into s.readback
+// and waits for them: a kernel writes them to mapped host memory, so the
+// read does not wait for copies that other streams have queued on the copy
+// engines (the host pipeline keeps multi-GB result copies in flight while
+// the next batch is matched).
+const uint32_t *read_back(MatchScratch &s, const void *a, uint32_t na, const void *b, uint32_t nb, cudaStream_t st) {
+    s.readback.reserve(size_t(na) + nb);
+    const unsigned blocks = std::min(64u, (na + nb + 255) / 256);
+    k_readback<<<std::max(blocks, 1u), 256, 0, st>>>(static_cast<const uint32_t *>(a), na,
+                                                     static_cast<const uint32_t *>(b), nb, s.readback.d);
+    TM_CHECK_LAUNCH();
+    TM_CUDA(cudaStreamSynchronize(st));
+    return s.readback.h;
 }
 
 MatchScratch::~MatchScratch() {
@@ -131,15 +148,14 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         TM_CHECK_LAUNCH();
     }
     exclusive_scan<uint32_t, uint32_t>(s.part_count.p, s.part_off.p, P, s.scr, st);
-    uint32_t routed = 0;
     s.h_part_count.resize(P);
-    TM_CUDA(cudaMemcpyAsync(&routed, s.part_off.p + P, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    TM_CUDA(cudaMemcpyAsync(s.h_part_count.data(), s.part_count.p, P * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    TM_CUDA(cudaStreamSynchronize(st));
+    const uint32_t *rb = read_back(s, s.part_count.p, P, s.part_off.p + P, 1, st);
+    std::copy(rb, rb + P, s.h_part_count.begin());
+    const uint32_t routed = rb[P];
     bs.routed = routed;
     for (uint32_t p = 0; p < P; ++p) bs.dense += uint64_t(s.h_part_count[p]) * t.h_part_size[p];
     const uint32_t windows = (P + kMaxRouteParts - 1) / kMaxRouteParts;
-    bs.launches += 2 * windows + 2 + scan_launches(P);  // route x2, slices, match, scan
+    bs.launches += 2 * windows + 3 + scan_launches(P);  // route x2, readback, slices, match, scan
     s.queue.reserve(size_t(std::max<uint32_t>(routed, 1)) * kQueueWords + kChunk * kQueueWords);
     for (uint32_t p0 = 0; p0 < P; p0 += kMaxRouteParts) {
         const uint32_t pw = std::min(kMaxRouteParts, P - p0);
@@ -199,8 +215,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         TM_CHECK_LAUNCH();
         if (s.profile) TM_CUDA(cudaEventRecord(s.ev_end, st));
         if (match_end) TM_CUDA(cudaEventRecord(match_end, st));
-        TM_CUDA(cudaMemcpyAsync(hc, s.counters.p, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-        TM_CUDA(cudaStreamSynchronize(st));
+        std::memcpy(hc, read_back(s, s.counters.p, 6, nullptr, 0, st), 3 * sizeof(unsigned long long));
         if (hc[2]) throw Error(TM_ERR_TIMEOUT, "match kernel: bounded wait for the query copy expired");
         if (work_counters) {
             unsigned long long w[8];
@@ -223,13 +238,13 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     // ---- keys ----
     TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
     const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256), unsigned(s.sm_count) * 16));
-    bs.launches += 2 + scan_launches(nq) + uint32_t(bs.retries);
+    // pair-count readback, count, fill, key-total readback; each retry: match + readback
+    bs.launches += 4 + scan_launches(nq) + 2 * uint32_t(bs.retries);
     k_key_count<<<gblocks, 256, 0, st>>>(s.pairs.p, s.counters.p, t.slot_key_off.p, s.qkeys.p);
     TM_CHECK_LAUNCH();
     exclusive_scan<uint32_t, uint64_t>(s.qkeys.p, s.qoff.p, nq, s.scr, st);
     uint64_t total = 0;
-    TM_CUDA(cudaMemcpyAsync(&total, s.qoff.p + nq, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-    TM_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(&total, read_back(s, s.qoff.p + nq, 2, nullptr, 0, st), sizeof(uint64_t));
     s.keys.reserve(std::max<uint64_t>(total, 1));
     s.qcursor.reserve(nq);
     TM_CUDA(cudaMemsetAsync(s.qcursor.p, 0, nq * sizeof(uint32_t), st));
@@ -257,13 +272,12 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     }
     TM_CHECK_LAUNCH();
     exclusive_scan<uint32_t, uint64_t>(s.ucount.p, s.uoff.p, nq, s.scr, st);
-    uint64_t utotal = 0;
-    TM_CUDA(cudaMemcpyAsync(&utotal, s.uoff.p + nq, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
     // compact into s.keys (unique prefix of every segment is <= its length)
     k_compact<<<nq, 256, 0, st>>>(s.ukeys.p, s.qoff.p, s.uoff.p, nq, s.keys.p);
-    bs.launches += 2 + scan_launches(nq);
+    bs.launches += 3 + scan_launches(nq);  // unique, compact, readback, scan
     TM_CHECK_LAUNCH();
-    TM_CUDA(cudaStreamSynchronize(st));
+    uint64_t utotal = 0;
+    std::memcpy(&utotal, read_back(s, s.uoff.p + nq, 2, nullptr, 0, st), sizeof(uint64_t));
     *d_offsets = s.uoff.p;
     *d_keys = s.keys.p;
     *n_keys = utotal;

@@ -29,6 +29,7 @@ struct MatchScratch {
     DevBuf<uint32_t> ucount;      // [nq]
     DevBuf<uint64_t> uoff;        // [nq + 1]
     DevBuf<uint32_t> ukeys;       // [total unique] (also radix temp)
+    MappedBuf<uint32_t> readback; // small device results read by the host (k_readback)
     std::vector<uint32_t> h_part_count, h_chunk_off, h_item_off;
     ScanScratch scr;
     int sm_count = 0;

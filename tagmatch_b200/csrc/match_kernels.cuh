@@ -587,6 +587,16 @@ __global__ void k_compact(const uint32_t *__restrict__ ukeys, const uint64_t *__
     for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) out[dst + i] = ukeys[src + i];
 }
 
+// Copies na words at a, then nb words at b, into mapped pinned host memory
+// (dst is its device view).  Used for the few numbers the host needs in the
+// middle of a batch (queue sizes, pair and key totals).
+__global__ void k_readback(const uint32_t *__restrict__ a, uint32_t na, const uint32_t *__restrict__ b, uint32_t nb,
+                           uint32_t *__restrict__ dst) {
+    const uint32_t n = na + nb;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = i < na ? a[i] : b[i - na];
+}
+
 // Keys narrowed to 16 bits for the trip to the host (tables whose largest
 // key is below 65,536); the host widens them back.
 __global__ void k_narrow16(const uint32_t *__restrict__ in, uint64_t n, uint16_t *__restrict__ out) {

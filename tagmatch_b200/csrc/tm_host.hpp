@@ -106,4 +106,56 @@ struct HostBuf {
     }
 };
 
+// Pinned host buffer mapped into the device address space (grow-only).
+// Kernels store small results into it (d); the host reads them (h) after a
+// stream synchronisation.  Such stores leave the SMs over PCIe directly, so
+// unlike a cudaMemcpyAsync they do not queue on a copy engine behind large
+// copies that other streams have issued.
+template <class T>
+struct MappedBuf {
+    T *h = nullptr;
+    T *d = nullptr;
+    size_t cap = 0;
+    MappedBuf() = default;
+    MappedBuf(const MappedBuf &) = delete;
+    MappedBuf &operator=(const MappedBuf &) = delete;
+    MappedBuf(MappedBuf &&o) noexcept : h(o.h), d(o.d), cap(o.cap) {
+        o.h = o.d = nullptr;
+        o.cap = 0;
+    }
+    MappedBuf &operator=(MappedBuf &&o) noexcept {
+        if (this != &o) {
+            release();
+            h = o.h;
+            d = o.d;
+            cap = o.cap;
+            o.h = o.d = nullptr;
+            o.cap = 0;
+        }
+        return *this;
+    }
+    ~MappedBuf() { release(); }
+    void reserve(size_t n) {
+        if (n <= cap && h) return;
+        if (h) n = std::max(n, cap + cap / 2);
+        release();
+        const size_t bytes = (n ? n : 1) * sizeof(T);
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&h), bytes, cudaHostAllocMapped);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer(reinterpret_cast<void **>(&d), h, 0);
+        if (e != cudaSuccess) {
+            if (h) cudaFreeHost(h);
+            h = d = nullptr;
+            cap = 0;
+            cudaGetLastError();
+            throw Error(-5, cuda_msg(e, "cudaHostAlloc(mapped)", __FILE__, __LINE__));
+        }
+        cap = n ? n : 1;
+    }
+    void release() {
+        if (h) cudaFreeHost(h);
+        h = d = nullptr;
+        cap = 0;
+    }
+};
+
 }  // namespace tmb
