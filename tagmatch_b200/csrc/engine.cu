@@ -409,8 +409,8 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
         TM_CUDA(cudaMemcpyAsync(ln.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, ln.stream));
         if (nk) TM_CUDA(cudaMemcpyAsync(ln.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, ln.stream));
         TM_CUDA(cudaStreamSynchronize(ln.stream));
-        // running estimate of device bytes per query (queues, pairs, keys)
-        const uint64_t bytes = bs.routed * (kQueueWords * 4) + bs.pairs * sizeof(Pair) + nk * 4 * (unique ? 3 : 1);
+        // running estimate of device bytes per query (queues, hit records, keys)
+        const uint64_t bytes = bs.routed * (kQueueWords * 4) + bs.records * sizeof(HitRec) + nk * 4 * (unique ? 3 : 1);
         const uint64_t bpq = std::max<uint64_t>(1024, bytes / std::max<uint32_t>(nq, 1));
         bytes_per_query_.store((bytes_per_query_.load() * 3 + bpq) / 4);
     } catch (const Error &e) {

@@ -29,13 +29,17 @@
 //                registers; the tile's AND mask selects candidate queries by
 //                OR-ing the slices of its bits (8 lanes, one 32-query word
 //                each); each candidate is tested against the 32 filters with
-//                6 LOP3s; hits are compacted with ballot/popc into a
+//                6 LOP3s; a ballot per candidate gives the tile's hit mask
+//                for that query, staged as a (query, tile, mask) record in a
 //                per-warp shared-memory buffer flushed with one global atomic;
-//   k_key_count / k_key_fill   per-query key counts (warp-aggregated atomics
-//                over lanes holding the same query), prefix sums, key copy;
+//   k_key_count  per record: its key total (a run of adjacent hit bits is
+//                one key range of the tile's slots), added to the query's;
+//   k_key_fill   after a prefix sum of the query totals: one cursor atomic
+//                per group of same-query records in a warp, then one
+//                contiguous key range per run of hit bits;
 //   k_unique_*   match_unique: per-query bitmap (small key spaces, output
 //                comes out sorted) or per-query block radix sort + unique.
-// Result overflow is exact: the pair buffer is regrown and the batch re-run
+// Result overflow is exact: the record buffer is regrown and the batch re-run
 // (the reference truncates silently at 4,194,304 hits, gpu.cu:55).
 #include "match_kernels.cuh"
 #include <cstdio>
@@ -57,7 +61,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     work = std::move(o.work);
     keys16 = std::move(o.keys16);
     counters = std::move(o.counters);
-    pairs = std::move(o.pairs);
+    recs = std::move(o.recs);
     qkeys = std::move(o.qkeys);
     qoff = std::move(o.qoff);
     qcursor = std::move(o.qcursor);
@@ -68,7 +72,7 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     readback = std::move(o.readback);
     for (int i = 0; i < 2 * ScanScratch::kLevels; ++i) scr.levels[i] = std::move(o.scr.levels[i]);
     sm_count = o.sm_count;
-    pair_cap_hint = o.pair_cap_hint;
+    rec_cap_hint = o.rec_cap_hint;
     seg_tiles = o.seg_tiles;
     profile = o.profile;
     if (ev_begin) cudaEventDestroy(ev_begin);
@@ -189,8 +193,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     }
     bs.items = items;
     // ---- match (regrow and re-run on pair overflow) ----
-    if (s.pair_cap_hint == 0) s.pair_cap_hint = size_t(nq) * 1024 + (1u << 20);
-    s.pairs.reserve(s.pair_cap_hint);
+    if (s.rec_cap_hint == 0) s.rec_cap_hint = size_t(nq) * 512 + (1u << 20);
+    s.recs.reserve(s.rec_cap_hint);
     unsigned long long hc[4] = {0, 0, 0, 0};
     for (int attempt = 0;; ++attempt) {
         TM_CUDA(cudaMemsetAsync(s.counters.p, 0, 4 * sizeof(unsigned long long), st));
@@ -200,8 +204,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             TM_CUDA(cudaMemsetAsync(s.work.p, 0, 8 * sizeof(unsigned long long), st));
         }
         MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, s.part_count.p, s.part_off.p, s.item_off.p,
-                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p, s.pairs.p,
-                    (unsigned long long)s.pairs.cap, work_counters ? s.work.p : nullptr};
+                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p, s.recs.p,
+                    (unsigned long long)s.recs.cap, work_counters ? s.work.p : nullptr};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
             if (!s.ev_begin) {
@@ -215,12 +219,14 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         TM_CHECK_LAUNCH();
         if (s.profile) TM_CUDA(cudaEventRecord(s.ev_end, st));
         if (match_end) TM_CUDA(cudaEventRecord(match_end, st));
-        std::memcpy(hc, read_back(s, s.counters.p, 6, nullptr, 0, st), 3 * sizeof(unsigned long long));
+        std::memcpy(hc, read_back(s, s.counters.p, 8, nullptr, 0, st), 4 * sizeof(unsigned long long));
         if (hc[2]) throw Error(TM_ERR_TIMEOUT, "match kernel: bounded wait for the query copy expired");
         if (work_counters) {
             unsigned long long w[8];
             TM_CUDA(cudaMemcpy(w, s.work.p, sizeof(w), cudaMemcpyDeviceToHost));
-            std::fprintf(stderr, "[tm work] queries %u tile_visits %llu and_bits %llu candidates %llu trips %llu items %llu pairs %llu\n",
+            std::fprintf(stderr,
+                         "[tm work] queries %u tile_visits %llu and_bits %llu candidates %llu trips %llu items %llu "
+                         "records %llu\n",
                          nq, w[0], w[1], w[2], w[3], w[4], hc[1]);
         }
         if (s.profile) {
@@ -228,27 +234,31 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             TM_CUDA(cudaEventElapsedTime(&ms, s.ev_begin, s.ev_end));
             bs.match_ms += ms;
         }
-        if (hc[1] <= s.pairs.cap) break;
-        if (attempt >= 3) throw Error(TM_ERR_INTERNAL, "pair buffer regrowth did not converge");
-        s.pair_cap_hint = size_t(hc[1] + hc[1] / 4 + 1024);
-        s.pairs.reserve(s.pair_cap_hint);
+        if (hc[1] <= s.recs.cap) break;
+        if (attempt >= 3) throw Error(TM_ERR_INTERNAL, "hit record buffer regrowth did not converge");
+        s.rec_cap_hint = size_t(hc[1] + hc[1] / 4 + 1024);
+        s.recs.reserve(s.rec_cap_hint);
         bs.retries++;
     }
-    bs.pairs = hc[1];
+    bs.records = hc[1];
     // ---- keys ----
-    TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
     const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256), unsigned(s.sm_count) * 16));
-    // pair-count readback, count, fill, key-total readback; each retry: match + readback
+    // record-count readback, count, fill, key-total readback; each retry: match + readback
     bs.launches += 4 + scan_launches(nq) + 2 * uint32_t(bs.retries);
-    k_key_count<<<gblocks, 256, 0, st>>>(s.pairs.p, s.counters.p, t.slot_key_off.p, s.qkeys.p);
+    TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
+    k_key_count<<<gblocks, 256, 0, st>>>(s.recs.p, s.counters.p, t.slot_key_off.p, s.qkeys.p);
     TM_CHECK_LAUNCH();
     exclusive_scan<uint32_t, uint64_t>(s.qkeys.p, s.qoff.p, nq, s.scr, st);
-    uint64_t total = 0;
-    std::memcpy(&total, read_back(s, s.qoff.p + nq, 2, nullptr, 0, st), sizeof(uint64_t));
+    // key total and matching pairs (k_key_count's count in counters[3])
+    uint64_t total = 0, pairs = 0;
+    const uint32_t *tb = read_back(s, s.qoff.p + nq, 2, s.counters.p + 3, 2, st);
+    std::memcpy(&total, tb, sizeof(uint64_t));
+    std::memcpy(&pairs, tb + 2, sizeof(uint64_t));
+    bs.pairs = pairs;
     s.keys.reserve(std::max<uint64_t>(total, 1));
     s.qcursor.reserve(nq);
     TM_CUDA(cudaMemsetAsync(s.qcursor.p, 0, nq * sizeof(uint32_t), st));
-    k_key_fill<<<gblocks, 256, 0, st>>>(s.pairs.p, s.counters.p, t.slot_key_off.p, t.keys.p, s.qoff.p, s.qcursor.p, s.keys.p);
+    k_key_fill<<<gblocks, 256, 0, st>>>(s.recs.p, s.counters.p, t.slot_key_off.p, t.keys.p, s.qoff.p, s.qcursor.p, s.keys.p);
     TM_CHECK_LAUNCH();
     if (!unique) {
         TM_CUDA(cudaStreamSynchronize(st));

@@ -20,8 +20,8 @@ struct MatchScratch {
     DevBuf<uint32_t> slices;      // [chunks][192][8] bit-sliced "lacks bit" masks
     DevBuf<unsigned long long> work;  // optional kernel work counters
     DevBuf<uint16_t> keys16;          // keys narrowed for the host transfer
-    DevBuf<unsigned long long> counters;  // [0] work item, [1] pairs, [2] error flags
-    DevBuf<Pair> pairs;
+    DevBuf<unsigned long long> counters;  // [0] work item, [1] hit records, [2] error flags, [3] pairs
+    DevBuf<HitRec> recs;          // hit records of the subset test
     DevBuf<uint32_t> qkeys;       // [nq]
     DevBuf<uint64_t> qoff;        // [nq + 1]
     DevBuf<uint32_t> qcursor;     // [nq]
@@ -33,7 +33,7 @@ struct MatchScratch {
     std::vector<uint32_t> h_part_count, h_chunk_off, h_item_off;
     ScanScratch scr;
     int sm_count = 0;
-    size_t pair_cap_hint = 0;
+    size_t rec_cap_hint = 0;
     uint32_t seg_tiles = kSegTiles;  // tiles per work item
     // optional CUDA-event timing of the subset-test kernel
     bool profile = false;
@@ -50,6 +50,7 @@ struct BatchStats {
     uint64_t routed = 0;   // (query, partition) pairs
     uint64_t items = 0;    // work items
     uint64_t pairs = 0;    // matching (query, filter) pairs
+    uint64_t records = 0;  // hit records ((query, tile) with at least one match)
     uint64_t keys = 0;     // output keys
     int retries = 0;       // pair-buffer regrowths
     float match_ms = 0.f;  // subset-test kernel time (profiling on)

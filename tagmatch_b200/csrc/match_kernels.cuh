@@ -12,7 +12,7 @@ namespace {
 constexpr int kRouteThreads = 256;
 constexpr int kMatchThreads = 256;
 constexpr int kMatchWarps = kMatchThreads / 32;
-constexpr int kWarpBuf = 128;  // staged pairs per warp
+constexpr int kWarpRecs = 64;  // staged hit records per warp (1 KB)
 constexpr uint32_t kMaxRouteParts = 1536;  // partition masks per routing window (48 KB of shared memory)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
@@ -154,9 +154,11 @@ struct MatchArgs {
     const uint32_t *slices;
     uint32_t n_parts;
     uint32_t seg_tiles;            // tiles per work item
-    unsigned long long *counters;  // [0] next item, [1] pairs, [2] error flags
-    Pair *pairs;
-    unsigned long long pair_cap;
+    // [0] next item, [1] hit records, [2] error flags, [3] matching
+    // (query, filter) pairs
+    unsigned long long *counters;
+    HitRec *recs;
+    unsigned long long rec_cap;
     // optional work counters (diagnostics): [0] tile visits, [1] AND-mask
     // bits OR-ed, [2] candidate (query, tile) pairs, [3] candidate loop
     // trips, [4] items; null when off
@@ -166,17 +168,24 @@ struct MatchArgs {
 constexpr int kSliceWords = kSliceRows * 8;  // 193 x 256 bits
 
 // One staging buffer: a chunk's query records and slices.
+// The query array has one record past the chunk: the pad record (all
+// words zero, query id kPadQuery) that candidate-list padding points at.
+constexpr uint32_t kPadQuery = 0xFFFFFFFFu;
 struct __align__(128) Stage {
-    uint32_t q[kChunk * kQueueWords];  // 8 KB
-    uint32_t z[kSliceWords];           // 6 KB
+    uint32_t q[(kChunk + 1) * kQueueWords];  // 8 KB + the pad record
+    uint32_t z[kSliceWords];                 // 6 KB
 };
 
-__device__ __forceinline__ void flush_warp(Pair *buf, uint32_t n, const MatchArgs &a, unsigned lane) {
+// Moves a warp's n staged records to the global record buffer (one atomic
+// reserves their place; past the capacity they are only counted, and the
+// host re-runs the batch with a larger buffer).
+__device__ __forceinline__ void flush_recs(HitRec *buf, uint32_t n, const MatchArgs &a, unsigned lane) {
+    __syncwarp();
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(&a.counters[1], (unsigned long long)n);
     base = __shfl_sync(kFull, base, 0);
-    if (base + n <= a.pair_cap) {
-        for (uint32_t i = lane; i < n; i += 32) a.pairs[base + i] = buf[i];
+    if (base + n <= a.rec_cap) {
+        for (uint32_t i = lane; i < n; i += 32) a.recs[base + i] = buf[i];
     }
     __syncwarp();
 }
@@ -239,16 +248,19 @@ __device__ __forceinline__ void produce(const MatchArgs &a, uint32_t total, Stag
 
 // COUNT: diagnostics instantiation that also tallies its work (a.work).
 template <bool COUNT>
-__global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
+__global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4 CTAs per SM: up to 64 registers
     __shared__ Stage st[2];
-    __shared__ __align__(16) Pair s_out[kMatchWarps][kWarpBuf];
+    __shared__ __align__(16) HitRec s_rec[kMatchWarps][kWarpRecs];
     __shared__ __align__(16) uint32_t s_list[kMatchWarps][kChunk + 4];  // per-warp candidate lists
-    __shared__ uint32_t s_nout[kMatchWarps];                             // pairs staged per warp
     __shared__ __align__(8) uint64_t full[2], empty[2];
     __shared__ uint32_t s_item[2];
     __shared__ int s_fail;
     const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t total = a.item_off[a.n_parts];
+    if (tid < 2 * kQueueWords) {
+        const uint32_t k = tid % kQueueWords;
+        st[tid / kQueueWords].q[kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
+    }
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
@@ -257,10 +269,11 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
-    if (tid < kMatchWarps) s_nout[tid] = 0;
     __syncthreads();
     if (tid == 0) produce(a, total, st, full, s_item, 0);
     uint32_t w_tiles = 0, w_bits = 0, w_cand = 0, w_trips = 0, w_items = 0;
+    uint32_t wn = 0;  // records staged by this warp (warp-uniform)
+    const uint32_t lane_lt = (1u << lane) - 1u;
     for (uint32_t it = 0;; ++it) {
         const int b = it & 1;
         // prefetch the next item into the other stage once every warp has
@@ -271,12 +284,14 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
             if (ok) produce(a, total, st, full, s_item, b ^ 1);
             else { atomicOr(&a.counters[2], 1ull); s_fail = 1; }
         }
-        if (!mbar_wait(&full[b], (it >> 1) & 1)) {
-            atomicOr(&a.counters[2], 2ull);
+        // every exit is taken by whole warps (record flushes use the full warp)
+        const bool got = mbar_wait(&full[b], (it >> 1) & 1);
+        if (!__all_sync(kFull, got)) {
+            if (lane == 0) atomicOr(&a.counters[2], 2ull);
             break;
         }
         const uint32_t item = s_item[b];
-        if (item >= total || s_fail) break;
+        if (__any_sync(kFull, item >= total || s_fail)) break;
         const ItemRef r = locate(a, item);
         if (COUNT) ++w_items;
         const uint4 *sq = reinterpret_cast<const uint4 *>(st[b].q);
@@ -287,6 +302,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
             for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
             const TileInfo ti = a.tile_info[t];
             const bool lane_valid = lane < ti.count;
+            const uint32_t vm = ti.count >= 32u ? kFull : (1u << ti.count) - 1u;  // lanes holding a filter
             if (COUNT) ++w_tiles;
             // candidates: queries holding the tile's selection bits; lane
             // w < 8 ORs the "lacks" slices for queries 32 w .. 32 w + 31
@@ -320,7 +336,7 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
                     c &= c - 1;
                 }
             } else if (lane < 12) {
-                list[n + lane - 8] = 0;  // pad to a multiple of 4 with a valid index
+                list[n + lane - 8] = kChunk * 2;  // pad to a multiple of 4: the stage's pad record
             }
             __syncwarp();
             for (uint32_t i = 0; i < n; i += 4) {
@@ -351,48 +367,33 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
                 x1 = andnot_or(f[5], q1.y, x1);
                 x2 = andnot_or(f[5], r1.y, x2);
                 x3 = andnot_or(f[5], u1.y, x3);
-                // common case: no hit among the four (one min chain)
-                if (min(min(x0, x1), min(x2, x3)) != 0 || !lane_valid) continue;
-                const uint32_t hb = uint32_t(x0 == 0) | (uint32_t(x1 == 0 && i + 1 < n) << 1) |
-                                    (uint32_t(x2 == 0 && i + 2 < n) << 2) | (uint32_t(x3 == 0 && i + 3 < n) << 3);
-                if (hb) {
-                    // usually one lane with one hit: a shared-memory atomic
-                    // reserves its slots; slots past the buffer go to global
-                    const uint32_t c = __popc(hb);
-                    uint32_t pos = atomicAdd(&s_nout[warp], c);
-                    const uint32_t slot = t * kTile + lane;
-                    const uint32_t qid[4] = {p1.z, q1.z, r1.z, u1.z};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if ((hb >> k) & 1u) {
-                            const Pair pr{qid[k], slot};
-                            if (pos < (uint32_t)kWarpBuf) {
-                                s_out[warp][pos] = pr;
-                            } else {
-                                const unsigned long long g = atomicAdd(&a.counters[1], 1ull);
-                                if (g < a.pair_cap) a.pairs[g] = pr;
-                            }
-                            ++pos;
-                        }
-                    }
+                // common case: no hit among the four (one min chain, one vote)
+                if (!__any_sync(kFull, lane_valid && min(min(x0, x1), min(x2, x3)) == 0)) continue;
+                // warp-uniform from here: one ballot per candidate gives the
+                // tile's hit mask for that query; lane k < 4 stages record k
+                // (list padding reads the stage's pad record: query id
+                // kPadQuery, dropped by the key gather)
+                const uint32_t b0 = __ballot_sync(kFull, x0 == 0) & vm;
+                const uint32_t b1 = __ballot_sync(kFull, x1 == 0) & vm;
+                const uint32_t b2 = __ballot_sync(kFull, x2 == 0) & vm;
+                const uint32_t b3 = __ballot_sync(kFull, x3 == 0) & vm;
+                const uint32_t mine = lane == 0 ? b0 : lane == 1 ? b1 : lane == 2 ? b2 : b3;
+                const uint32_t qid = lane == 0 ? p1.z : lane == 1 ? q1.z : lane == 2 ? r1.z : u1.z;
+                const bool w = lane < 4 && mine != 0;
+                const uint32_t wm = __ballot_sync(kFull, w);
+                if (wn + 4 > (uint32_t)kWarpRecs) {
+                    flush_recs(s_rec[warp], wn, a, lane);
+                    wn = 0;
                 }
-            }
-            __syncwarp();
-            // flush the warp's buffer when it is more than half full
-            const uint32_t held = s_nout[warp];
-            if (held >= (uint32_t)kWarpBuf / 2) {
-                flush_warp(s_out[warp], min(held, (uint32_t)kWarpBuf), a, lane);
-                if (lane == 0) s_nout[warp] = 0;
-                __syncwarp();
+                if (w) s_rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qid, t, mine, 0u};
+                wn += __popc(wm);
             }
             __syncwarp();  // the list is rebuilt for the next tile
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[b]);
     }
-    __syncwarp();
-    const uint32_t held = s_nout[warp];
-    if (held) flush_warp(s_out[warp], min(held, (uint32_t)kWarpBuf), a, lane);
+    if (wn) flush_recs(s_rec[warp], wn, a, lane);
     if (COUNT && lane == 0) {
         atomicAdd(&a.work[0], (unsigned long long)w_tiles);
         atomicAdd(&a.work[1], (unsigned long long)w_bits);
@@ -405,9 +406,46 @@ __global__ void __launch_bounds__(kMatchThreads) k_match(MatchArgs a) {
 // ---------------------------------------------------------------------------
 // Key gather
 // ---------------------------------------------------------------------------
-// Lanes of a warp that hold pairs of the same query form one group
-// (__match_any_sync); each lane gets the sum of its group's key counts and
-// the part of it held by lower lanes, so a group needs one atomic.
+// Keys of the filters in a hit mask.  The table keeps keys in slot order, so
+// a run of adjacent set bits [lo, hi) is the one key range [o[lo], o[hi])
+// (o: the tile's slot key offsets, 33 of them).  Calls f(begin, end) per run.
+template <class F>
+__device__ __forceinline__ void for_each_key_run(const uint32_t *__restrict__ o, uint32_t mask, F f) {
+    uint64_t m = mask;
+    while (m) {
+        const int lo = __ffsll(m) - 1;
+        const uint64_t filled = m + (1ull << lo);  // the carry clears the run and sets bit hi
+        const int hi = __ffsll(filled & ~m) - 1;
+        f(o[lo], o[hi]);
+        m &= filled;
+    }
+}
+
+// Per-query key totals (qkeys, zeroed by the caller), one atomic per
+// record; each record keeps its own total in nkeys for the fill.  Also
+// counts the matching (query, filter) pairs (counters[3]).  Records of the
+// pad query (candidate-list padding) are skipped.
+__global__ void k_key_count(HitRec *__restrict__ recs, unsigned long long *__restrict__ counters,
+                            const uint32_t *__restrict__ slot_key_off, uint32_t *__restrict__ qkeys) {
+    const unsigned long long n = counters[1];
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    uint32_t pairs = 0;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const HitRec r = recs[i];
+        if (r.query == kPadQuery) continue;
+        uint32_t nk = 0;
+        for_each_key_run(slot_key_off + size_t(r.tile) * kTile, r.mask, [&](uint32_t b, uint32_t e) { nk += e - b; });
+        recs[i].nkeys = nk;
+        atomicAdd(&qkeys[r.query], nk);
+        pairs += __popc(r.mask);
+    }
+    pairs = __reduce_add_sync(kFull, pairs);
+    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&counters[3], (unsigned long long)pairs);
+}
+
+// Lanes of a warp holding records of the same query form one group
+// (__match_any_sync): each lane gets the sum of its group's key totals and
+// the part of it held by lower lanes, so a group needs one cursor atomic.
 __device__ __forceinline__ void group_sums(uint32_t peers, uint32_t nk, unsigned lane, uint32_t &excl, uint32_t &tot) {
     excl = 0;
     tot = 0;
@@ -421,29 +459,11 @@ __device__ __forceinline__ void group_sums(uint32_t peers, uint32_t nk, unsigned
     }
 }
 
-__global__ void k_key_count(const Pair *__restrict__ pairs, const unsigned long long *__restrict__ counters,
-                            const uint32_t *__restrict__ slot_key_off, uint32_t *__restrict__ qkeys) {
-    const unsigned long long n = counters[1];
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
-    for (unsigned long long base = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x - lane); base < n;
-         base += warps * 32) {
-        const unsigned long long i = base + lane;
-        const bool valid = i < n;
-        Pair pr{0xFFFFFFFFu, 0u};
-        uint32_t nk = 0;
-        if (valid) {
-            pr = pairs[i];
-            nk = slot_key_off[pr.slot + 1] - slot_key_off[pr.slot];
-        }
-        const uint32_t peers = __match_any_sync(kFull, pr.query);
-        uint32_t excl, tot;
-        group_sums(peers, nk, lane, excl, tot);
-        if (valid && lane == (unsigned)(__ffs(peers) - 1) && tot) atomicAdd(&qkeys[pr.query], tot);
-    }
-}
-
-__global__ void k_key_fill(const Pair *__restrict__ pairs, const unsigned long long *__restrict__ counters,
+// Copies every record's keys into its query's range (qoff): a group of
+// same-query records reserves its keys with one atomic on the query's
+// cursor (qcursor, zeroed by the caller), then each record copies one
+// contiguous key range per run of hit bits.
+__global__ void k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
                            const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
                            const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor, uint32_t *__restrict__ out) {
     const unsigned long long n = counters[1];
@@ -452,22 +472,20 @@ __global__ void k_key_fill(const Pair *__restrict__ pairs, const unsigned long l
     for (unsigned long long base = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x - lane); base < n;
          base += warps * 32) {
         const unsigned long long i = base + lane;
-        const bool valid = i < n;
-        Pair pr{0xFFFFFFFFu, 0u};
-        uint32_t b = 0, e = 0;
-        if (valid) {
-            pr = pairs[i];
-            b = slot_key_off[pr.slot];
-            e = slot_key_off[pr.slot + 1];
-        }
-        const uint32_t peers = __match_any_sync(kFull, pr.query);
+        HitRec r{kPadQuery, 0u, 0u, 0u};
+        if (i < n) r = recs[i];
+        const uint32_t nk = r.query == kPadQuery ? 0u : r.nkeys;
+        const uint32_t peers = __match_any_sync(kFull, r.query);
         uint32_t excl, tot;
-        group_sums(peers, e - b, lane, excl, tot);
+        group_sums(peers, nk, lane, excl, tot);
         const unsigned leader = __ffs(peers) - 1;
         uint64_t pos = 0;
-        if (valid && lane == leader && tot) pos = qoff[pr.query] + atomicAdd(&qcursor[pr.query], tot);
-        pos = __shfl_sync(kFull, pos, leader) + excl;
-        for (uint32_t k = b; k < e; ++k) out[pos++] = tkeys[k];
+        if (lane == leader && tot) pos = qoff[r.query] + atomicAdd(&qcursor[r.query], tot);
+        uint32_t *dst = out + __shfl_sync(kFull, pos, leader) + excl;
+        if (nk)
+            for_each_key_run(slot_key_off + size_t(r.tile) * kTile, r.mask, [&](uint32_t b, uint32_t e) {
+                for (uint32_t k = b; k < e; ++k) *dst++ = tkeys[k];
+            });
     }
 }
 

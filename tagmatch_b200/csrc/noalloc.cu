@@ -187,26 +187,26 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         k_slices<<<chunks, kChunk, 0, st>>>(queue, part_off, part_count, chunk_off, P, slices);
         TM_CHECK_LAUNCH();
     }
-    // matching pairs fill what is left of the array (a quarter of it is
-    // kept back for the match_unique key buffer)
-    const size_t pair_room = (unique ? ar.left() * 3 / 4 : ar.left()) / sizeof(Pair);
-    if (pair_room < 256) throw Error(TM_ERR_CAPACITY, "no-allocation scratch exhausted before the pair buffer; split the batch");
-    Pair *pairs = ar.take<Pair>(pair_room - 32, "matching pairs");
+    // hit records fill what is left of the array (a quarter of it is kept
+    // back for the match_unique key buffer)
+    const size_t rec_room = (unique ? ar.left() * 3 / 4 : ar.left()) / sizeof(HitRec);
+    if (rec_room < 256) throw Error(TM_ERR_CAPACITY, "no-allocation scratch exhausted before the hit records; split the batch");
+    HitRec *recs = ar.take<HitRec>(rec_room - 32, "hit records");
     MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, part_count, part_off, item_off, chunk_off, queue, slices,
-                P, uint32_t(kSegTiles), counters, pairs, (unsigned long long)(pair_room - 32), nullptr};
+                P, uint32_t(kSegTiles), counters, recs, (unsigned long long)(rec_room - 32), nullptr};
     k_match<false><<<unsigned(sms) * 4, kMatchThreads, 0, st>>>(a);
     TM_CHECK_LAUNCH();
     unsigned long long hc[3] = {0, 0, 0};
     TM_CUDA(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
     TM_CUDA(cudaStreamSynchronize(st));
     if (hc[2]) throw Error(TM_ERR_TIMEOUT, "match kernel: bounded wait for the query copy expired");
-    if (hc[1] > pair_room - 32)
+    if (hc[1] > rec_room - 32)
         throw Error(TM_ERR_CAPACITY, "no-allocation scratch too small for the " + std::to_string(hc[1]) +
-                                         " matching (query, filter) pairs of this batch; split the batch");
+                                         " hit records of this batch; split the batch");
 
     // keys
     const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256), unsigned(sms) * 16));
-    k_key_count<<<gblocks, 256, 0, st>>>(pairs, counters, t.slot_key_off.p, qkeys);
+    k_key_count<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, qkeys);
     TM_CHECK_LAUNCH();
     uint64_t *key_off = unique ? qoff : d_out_offsets;
     scan_fixed<uint32_t, uint64_t>(qkeys, key_off, nq, sums, offs, st);
@@ -217,7 +217,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         *n_keys = total;
         if (total > capacity)
             throw Error(TM_ERR_CAPACITY, "output key buffer too small: " + std::to_string(total) + " keys needed");
-        k_key_fill<<<gblocks, 256, 0, st>>>(pairs, counters, t.slot_key_off.p, t.keys.p, d_out_offsets, qcursor, d_out_keys);
+        k_key_fill<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, t.keys.p, d_out_offsets, qcursor, d_out_keys);
         TM_CHECK_LAUNCH();
         TM_CUDA(cudaStreamSynchronize(st));
         return;
@@ -228,7 +228,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     const bool bitmap = bitmap_words * 4 <= 48 * 1024;
     uint32_t *keys = ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
     uint32_t *ukeys = ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
-    k_key_fill<<<gblocks, 256, 0, st>>>(pairs, counters, t.slot_key_off.p, t.keys.p, qoff, qcursor, keys);
+    k_key_fill<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, t.keys.p, qoff, qcursor, keys);
     TM_CHECK_LAUNCH();
     if (bitmap) {
         k_unique_bitmap<<<nq, kUniqThreads, bitmap_words * 4, st>>>(keys, qoff, uint32_t(bitmap_words), ukeys, ucount);

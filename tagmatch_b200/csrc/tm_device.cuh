@@ -29,10 +29,14 @@ struct __align__(16) TileInfo {
     uint32_t partition;
 };
 
-// Matched (query, filter-slot) pair.
-struct __align__(8) Pair {
+// One candidate query's hits in one tile: bit l of mask is set when the
+// tile's filter in lane l (slot tile * 32 + l) matches the query.  nkeys is
+// filled in by the key count (the keys of those filters).
+struct __align__(16) HitRec {
     uint32_t query;
-    uint32_t slot;
+    uint32_t tile;
+    uint32_t mask;
+    uint32_t nkeys;
 };
 
 __device__ __forceinline__ uint32_t andnot_or(uint32_t f, uint32_t q, uint32_t acc) {
