@@ -265,7 +265,8 @@ def run_ours(args):
     # (24 B per filter streamed once per 256-query chunk, 24 B per routed
     # query, 8 B per matching pair) over its event-timed duration
     launches = max(st["match_kernel_launches"], 1)
-    alg_bytes = (st["dense_tests"] * 24 / 256 + st["routed"] * 24 + st["pairs"] * 8) / launches
+    # the partition's filters once per 256-query chunk, the queries, the hit records written
+    alg_bytes = (st["dense_tests"] * 24 / 256 + st["routed"] * 24 + st["records"] * 16) / launches
     kern_s = st["match_kernel_ms"] / 1e3 / launches
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kern_s / 1e9
@@ -300,6 +301,7 @@ def run_ours(args):
             "clocks": clocks, "gpu_launches": int(st["kernel_launches"]), "roofline": roofline,
             "matches": {"routed_per_query": round(st["routed"] / max(st["queries"], 1), 2),
                         "pairs_per_query": round(st["pairs"] / max(st["queries"], 1), 2),
+                        "hit_records_per_query": round(st["records"] / max(st["queries"], 1), 2),
                         "keys_per_query": round(st["keys"] / max(st["queries"], 1), 2)}}
 
     # ---- end to end through the host C ABI ----

@@ -200,7 +200,7 @@ int tm_get_table_info(tm_engine *e, tm_table_info *info);
 
 /* Cumulative statistics of the synchronous matcher: batches, queries,
  * routed (query, partition) pairs, work items, matching (query, filter)
- * pairs, output keys, pair-buffer regrowths; with profiling on, the
+ * pairs, output keys, hit-record buffer regrowths; with profiling on, the
  * subset-test kernel's launches and total time from CUDA events recorded
  * on its stream.  No reference counterpart (front_end::print_statistics,
  * front_end.cc:781-789, is the closest). */
@@ -213,6 +213,8 @@ typedef struct {
     uint64_t kernel_launches; /* all kernels launched by the matcher */
     uint64_t h2d_bytes, d2h_bytes; /* bytes copied by tm_match_batch (keys travel as 16 bits
                                       when every key of the table is below 65,536) */
+    uint64_t records; /* hit records written by the subset test: one per (query, tile of up to
+                         32 filters) with at least one match, 16 bytes each */
 } tm_match_stats;
 int tm_get_match_stats(tm_engine *e, tm_match_stats *st);
 int tm_reset_match_stats(tm_engine *e);

@@ -46,7 +46,7 @@ class MatchStats(ctypes.Structure):
                 ("pair_retries", ctypes.c_uint64), ("match_kernel_launches", ctypes.c_uint64),
                 ("match_kernel_ms", ctypes.c_double), ("dense_tests", ctypes.c_uint64),
                 ("kernel_launches", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64),
-                ("d2h_bytes", ctypes.c_uint64)]
+                ("d2h_bytes", ctypes.c_uint64), ("records", ctypes.c_uint64)]
 
 
 # name -> (restype, argtypes); every symbol include/tagmatch_b200.h declares

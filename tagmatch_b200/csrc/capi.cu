@@ -252,6 +252,7 @@ int tm_get_match_stats(tm_engine *e, tm_match_stats *st) {
     st->kernel_launches = s.launches;
     st->h2d_bytes = s.h2d_bytes;
     st->d2h_bytes = s.d2h_bytes;
+    st->records = s.records;
     return TM_OK;
 }
 

@@ -84,7 +84,7 @@ enum FlushMode : int {
 };
 
 struct EngineStats {
-    uint64_t batches = 0, queries = 0, routed = 0, items = 0, pairs = 0, keys = 0;
+    uint64_t batches = 0, queries = 0, routed = 0, items = 0, pairs = 0, keys = 0, records = 0;
     uint64_t pair_retries = 0;
     uint64_t match_launches = 0;
     double match_ms = 0.0;
@@ -96,6 +96,7 @@ struct EngineStats {
         routed += b.routed;
         items += b.items;
         pairs += b.pairs;
+        records += b.records;
         keys += b.keys;
         pair_retries += b.retries;
         dense += b.dense;
