@@ -636,6 +636,16 @@ void parallel_widen(uint32_t *dst, const uint16_t *src, uint64_t n) {
 constexpr double kDirectFraction = 0.1;
 // smallest batch of match_host's final, halving batches
 constexpr uint64_t kTailBatch = 4096;
+// output keys per match_host batch (about 2 GB narrowed, 4 GB wide): larger
+// batches let a batch's host copies fall behind the matching of the next
+// ones, and leave a long copy after the last match.  TM_HOST_BATCH_KEYS
+// overrides it (0: no cap).
+constexpr double kHostBatchKeys = double(1u << 30);
+
+double host_batch_keys() {
+    const char *s = std::getenv("TM_HOST_BATCH_KEYS");
+    return s && *s ? std::max(0.0, std::atof(s)) : kHostBatchKeys;
+}
 
 double direct_fraction() {
     const char *s = std::getenv("TM_DIRECT_FRACTION");
@@ -664,7 +674,7 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     TM_CUDA(cudaSetDevice(d.id));
     // TM_HOST_TRACE: one stderr line per batch with the host wait, match,
     // copy and widening times (diagnostics)
-    static const bool trace = std::getenv("TM_HOST_TRACE") != nullptr;
+    const bool trace = std::getenv("TM_HOST_TRACE") != nullptr;
     using TClock = std::chrono::steady_clock;
     const TClock::time_point t_call = TClock::now();
     auto ms_at = [&](TClock::time_point t) { return std::chrono::duration<double, std::milli>(t - t_call).count(); };
@@ -684,6 +694,7 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     const bool narrow = d.table.max_key < 65536u;
     const bool pinned_out = out_keys != nullptr && is_pinned(out_keys);
     const double frac = pinned_out ? direct_fraction() : 0.0;
+    const double batch_keys = host_batch_keys();
     struct Pending {
         bool active = false;
         uint64_t q0 = 0, base = 0, nk = 0, nd = 0;
@@ -719,11 +730,16 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     try {
         uint64_t it = 0;
         for (uint64_t q0 = 0, step = 0; q0 < nq; q0 += step, ++it) {
-            // full batches, then the last batch_limit_ queries in halving
-            // batches (down to kTailBatch): what is left to copy and widen
-            // after the last match is then a small batch's results
+            // batch size: the device batch limit, lowered so a batch's output
+            // stays near kHostBatchKeys keys (keys per query as last seen)
+            uint64_t full = batch_limit_;
+            if (host_keys_per_query_ > 0 && batch_keys > 0)
+                full = std::min<uint64_t>(full, std::max<uint64_t>(kTailBatch, uint64_t(batch_keys / host_keys_per_query_)));
+            // full batches, then the last `full` queries in halving batches
+            // (down to kTailBatch): what is left to copy and widen after the
+            // last match is then a small batch's results
             const uint64_t left = nq - q0;
-            step = left > batch_limit_ ? batch_limit_
+            step = left > full ? full
                    : left <= 2 * kTailBatch ? left
                                             : std::max<uint64_t>(kTailBatch, left / 2);
             const uint32_t n = uint32_t(step);
@@ -804,6 +820,7 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
                 overflow = true;
             }
             total += nk;
+            if (n >= kTailBatch) host_keys_per_query_ = double(nk) / n;
         }
         for (int l = 0; l < kHostLanes; ++l) finish(l);
     } catch (...) {

@@ -237,6 +237,7 @@ private:
     bool profile_ = false;
     int base_device_ = 0;
     uint32_t seg_tiles_ = kSegTiles;
+    double host_keys_per_query_ = 0;  // output keys per query of match_host's last batch
 
     // async path
     std::mutex q_mtx_;

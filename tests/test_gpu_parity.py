@@ -463,3 +463,38 @@ def test_latency_limit_flushes_without_stop():
     tm.stop()
     assert late.is_set()
     tm.close()
+
+
+def test_host_pipeline_pinned_output_and_direct_share():
+    """tm_match_batch into a pinned caller buffer.  Part of each batch's keys
+    is copied straight into that buffer as 32-bit values (TM_DIRECT_FRACTION),
+    the rest is narrowed to 16 bits and widened by the copy threads in
+    slices.  The batch limit is small, so batches outnumber the pipeline's
+    lanes and the final batches shrink.  Every split, and a table whose keys
+    need 32 bits, gives the same keys per query as the pageable path."""
+    import ctypes
+
+    import torch
+    f, ko, k = workload.generate_filters(20000, 5)
+    q = workload.generate_queries(12000, f, 5)
+    assert int(k.max()) < 65536  # the 16-bit transfer applies
+    for keys in (k, k + np.uint32(70000)):
+        tm = engine_with(f, ko, keys, 2000)
+        tm.set_batch_limit(1500)
+        ref_off, ref_keys = tm.match_batch(q)
+        n = q.shape[0]
+        out_keys = torch.empty(max(len(ref_keys), 1), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+        out_off = torch.empty(n + 1, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        lib = _native.load()
+        for frac in ("0", "0.3", "1"):
+            os.environ["TM_DIRECT_FRACTION"] = frac
+            try:
+                out_keys[:] = 0xDEADBEEF
+                nk = ctypes.c_uint64(0)
+                st = lib.tm_match_batch(tm._h, q.ctypes.data_as(_native.u32p), n, 0, out_off.ctypes.data_as(_native.u64p),
+                                        out_keys.ctypes.data_as(_native.u32p), out_keys.size, ctypes.byref(nk))
+            finally:
+                del os.environ["TM_DIRECT_FRACTION"]
+            assert st == 0 and nk.value == len(ref_keys)
+            assert_same_multisets(out_off.copy(), out_keys[: nk.value].copy(), ref_off, ref_keys)
+        tm.close()
