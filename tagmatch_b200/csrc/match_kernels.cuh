@@ -443,26 +443,13 @@ __global__ void k_key_count(HitRec *__restrict__ recs, unsigned long long *__res
     if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&counters[3], (unsigned long long)pairs);
 }
 
-// Lanes of a warp holding records of the same query form one group
-// (__match_any_sync): each lane gets the sum of its group's key totals and
-// the part of it held by lower lanes, so a group needs one cursor atomic.
-__device__ __forceinline__ void group_sums(uint32_t peers, uint32_t nk, unsigned lane, uint32_t &excl, uint32_t &tot) {
-    excl = 0;
-    tot = 0;
-#pragma unroll
-    for (int l = 0; l < 32; ++l) {
-        const uint32_t v = __shfl_sync(kFull, nk, l);
-        if ((peers >> l) & 1u) {
-            tot += v;
-            if ((unsigned)l < lane) excl += v;
-        }
-    }
-}
-
-// Copies every record's keys into its query's range (qoff): a group of
-// same-query records reserves its keys with one atomic on the query's
-// cursor (qcursor, zeroed by the caller), then each record copies one
-// contiguous key range per run of hit bits.
+// Copies every record's keys into its query's range (qoff).  Each lane
+// reserves its record's keys with one atomic on the query's cursor
+// (qcursor, zeroed by the caller).  Records whose hits form one run of
+// adjacent bits (the usual case) have one contiguous key range; the warp
+// copies those ranges together, 32 keys per step: a prefix sum over the
+// lanes' key counts, and for key j of the warp a 5-step shuffle search for
+// the lane that owns it.  Records with several runs copy their own ranges.
 __global__ void k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
                            const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
                            const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor, uint32_t *__restrict__ out) {
@@ -475,17 +462,44 @@ __global__ void k_key_fill(const HitRec *__restrict__ recs, const unsigned long 
         HitRec r{kPadQuery, 0u, 0u, 0u};
         if (i < n) r = recs[i];
         const uint32_t nk = r.query == kPadQuery ? 0u : r.nkeys;
-        const uint32_t peers = __match_any_sync(kFull, r.query);
-        uint32_t excl, tot;
-        group_sums(peers, nk, lane, excl, tot);
-        const unsigned leader = __ffs(peers) - 1;
-        uint64_t pos = 0;
-        if (lane == leader && tot) pos = qoff[r.query] + atomicAdd(&qcursor[r.query], tot);
-        uint32_t *dst = out + __shfl_sync(kFull, pos, leader) + excl;
-        if (nk)
-            for_each_key_run(slot_key_off + size_t(r.tile) * kTile, r.mask, [&](uint32_t b, uint32_t e) {
-                for (uint32_t k = b; k < e; ++k) *dst++ = tkeys[k];
+        const uint32_t *o = slot_key_off + size_t(r.tile) * kTile;
+        const uint32_t lo = nk ? uint32_t(__ffs(r.mask)) - 1 : 0u;
+        const uint32_t run = r.mask >> lo;
+        const bool single = nk && (run & (run + 1)) == 0;  // one run of adjacent bits
+        uint32_t src = single ? __ldg(&o[lo]) : 0u;
+        uint64_t dst = 0;
+        if (nk) dst = qoff[r.query] + atomicAdd(&qcursor[r.query], nk);
+        // several runs: this lane copies its own ranges
+        if (nk && !single) {
+            uint32_t *d = out + dst;
+            for_each_key_run(o, r.mask, [&](uint32_t b, uint32_t e) {
+                for (uint32_t k = b; k < e; ++k) *d++ = tkeys[k];
             });
+        }
+        // one run: the warp copies all such ranges together
+        const uint32_t cnk = single ? nk : 0u;
+        uint32_t incl = cnk;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, d);
+            if (lane >= (unsigned)d) incl += v;
+        }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t start = incl - cnk;  // this lane's first key among the warp's
+        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            // owner: the first lane whose inclusive count exceeds j
+            uint32_t owner = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
+                if (v <= j) owner += step;
+            }
+            const uint32_t ostart = __shfl_sync(kFull, start, owner);
+            const uint32_t osrc = __shfl_sync(kFull, src, owner);
+            const uint64_t odst = __shfl_sync(kFull, dst, owner);
+            if (j < total) out[odst + (j - ostart)] = tkeys[osrc + (j - ostart)];
+        }
     }
 }
 
