@@ -95,7 +95,9 @@ int tm_clear(tm_engine *e);
  * flushed; 0 means batches go out only when full or at stop(). */
 int tm_set_latency_limit_ms(tm_engine *e, uint32_t ms);
 uint32_t tm_get_latency_limit_ms(const tm_engine *e);
-/* Largest number of queries per device batch (default 65536). */
+/* Largest number of queries per device batch (default 65536).  tm_match_batch
+ * uses smaller batches when their results would exceed about 2^30 keys (from
+ * the keys per query of its previous batch), so result copies keep pace. */
 int tm_set_batch_limit(tm_engine *e, uint32_t queries);
 
 /* tagmatch::match / tagmatch::match_unique (tagmatch.cc:200-210) for a
@@ -106,7 +108,9 @@ int tm_set_batch_limit(tm_engine *e, uint32_t queries);
  * each query's keys sorted ascending without duplicates
  * (tagmatch_query.hh:99-119).  If capacity is too small, returns
  * TM_ERR_CAPACITY with the required key count in *n_keys (offsets are
- * complete).  Requires a consolidated table. */
+ * complete).  Requires a consolidated table.  Host buffers may be pageable;
+ * a pinned out_keys (cudaHostAlloc / cudaHostRegister) also receives part of
+ * the keys by direct DMA. */
 int tm_match_batch(tm_engine *e, const uint32_t *queries, uint64_t n, int unique, uint64_t *out_offsets,
                    uint32_t *out_keys, uint64_t capacity, uint64_t *n_keys);
 
@@ -164,7 +168,7 @@ int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uin
 #define TM_FLUSH_IMMEDIATE 1
 #define TM_FLUSH_SINGLE 2
 int tm_set_flush_mode(tm_engine *e, int mode);
-/* Device-memory budget per lane for a batch's queues, pairs and keys; the
+/* Device-memory budget per lane for a batch's queues, hit records and keys; the
  * number of queries admitted into one batch is capped by it (estimated
  * from the bytes per query of recent batches).  Default 16 GiB. */
 int tm_set_memory_budget(tm_engine *e, uint64_t bytes);
