@@ -400,17 +400,21 @@ def run_reference(args):
                 p.wait()
             return time.perf_counter() - t0
 
-        # table load time of test_matcher (no queries), subtracted from every step
-        t0 = time.perf_counter()
-        procs = [subprocess.Popen([oracle.REF_MATCHER, "F=" + fp, "Q=" + empty], stdout=subprocess.DEVNULL)
-                 for _ in range(cores)]
-        for p in procs:
-            p.wait()
-        t_load = time.perf_counter() - t0
-        # calibrate queries per process for ~10 s of matching per step
-        per = 2
-        t = run_shards(per, 0) - t_load
-        per = int(max(2, min(4096, per * 10.0 / max(t, 1e-3))))
+        # table load time of test_matcher (no queries), subtracted from every
+        # step; measured twice, the first run warming the file cache
+        for _ in range(2):
+            t0 = time.perf_counter()
+            procs = [subprocess.Popen([oracle.REF_MATCHER, "F=" + fp, "Q=" + empty], stdout=subprocess.DEVNULL)
+                     for _ in range(cores)]
+            for p in procs:
+                p.wait()
+            t_load = time.perf_counter() - t0
+        # calibrate queries per process for ~10 s of matching per step: a
+        # probe long enough (24 queries, ~1.6 s at 10M filters) to stand
+        # above the noise of the subtracted table load
+        probe = 24
+        t = max(run_shards(probe, 0) - t_load, 0.3)
+        per = int(max(8, min(512, probe * 10.0 / t)))
         for w in range(args.warmup):
             run_shards(per, (w + 1) * per * cores)
         times = []
