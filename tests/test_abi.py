@@ -105,3 +105,37 @@ int main() {
     subprocess.check_call(["g++", "-O1", "-std=c++17", "-I" + inc, str(src), "-o", str(exe)])
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
+
+
+def header_structs():
+    """name -> [(C type, field)] for every `typedef struct { ... } name;` in the header."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for body, name in re.findall(r"typedef struct \{(.*?)\}\s*(\w+);", src, flags=re.S):
+        fields = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            ctype, names = decl.split(None, 1)
+            fields += [(ctype, n.strip()) for n in names.split(",")]
+        out[name] = fields
+    return out
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the same fields, types
+    and order, and the same size as the C compiler gives them."""
+    ctypes_of = {"uint64_t": ctypes.c_uint64, "uint32_t": ctypes.c_uint32, "double": ctypes.c_double}
+    mirrors = {"tm_table_info": _native.TableInfo, "tm_match_stats": _native.MatchStats}
+    structs = header_structs()
+    assert set(mirrors) <= set(structs)
+    for cname, mirror in mirrors.items():
+        assert [(ctypes_of[t], n) for t, n in structs[cname]] == [(t, n) for n, t in mirror._fields_], cname
+    prog = tmp_path / "sizes.c"
+    prog.write_text('#include <stdio.h>\n#include "tagmatch_b200.h"\n'
+                    'int main(void) { printf("%zu %zu\\n", sizeof(tm_table_info), sizeof(tm_match_stats)); return 0; }\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(prog)], check=True)
+    sizes = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert sizes == [ctypes.sizeof(_native.TableInfo), ctypes.sizeof(_native.MatchStats)]
