@@ -185,7 +185,7 @@ int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p
 
 /* Autotuner (no reference counterpart): matches the n sample queries
  * [n][6] on device 0 with each candidate number of tiles per work item
- * (32..2,048) and device batch size (8,192..262,144, at most n), timed with
+ * (32..8,192) and device batch size (8,192..262,144, at most n), timed with
  * CUDA events, and keeps the fastest for this engine.  Reports the chosen
  * values and the sample's queries/s.  Results do not depend on either. */
 int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch_limit,

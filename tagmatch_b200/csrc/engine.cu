@@ -503,7 +503,7 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     TM_CUDA(cudaEventCreate(&e1));
     double best = -1.0;
     uint32_t best_seg = seg_tiles_, best_batch = batch_limit_;
-    const uint32_t segs[] = {32, 64, 128, 256, 512, 1024, 2048};
+    const uint32_t segs[] = {32, 64, 128, 256, 512, 1024, 2048, 4096, 8192};
     const uint32_t batches[] = {8192, 16384, 32768, 65536, 131072, 262144};
     try {
         for (uint32_t b : batches) {
