@@ -48,3 +48,30 @@ def test_two_gloo_ranks():
     for p, (o, e) in zip(procs, outs):
         assert p.returncode == 0, e[-2000:]
     assert "OK 11.0" in outs[0][0]
+
+
+def test_reference_arm_two_gloo_ranks():
+    """bench.py --impl reference under two ranks: rank 0 times the reference's
+    own matcher and prints one JSON line; rank 1 exits 0 without work."""
+    import json
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    if not os.path.exists(oracle.REF_MATCHER):
+        pytest.skip("reference matcher not built (oracle/_ref)")
+    port = _free_port()
+    procs = []
+    for r in range(2):
+        env = dict(os.environ, WORLD_SIZE="2", RANK=str(r), LOCAL_RANK=str(r), LOCAL_WORLD_SIZE="2",
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                                       "--steps", "1", "--warmup", "1", "--filters", "20000", "--queries", "4096"],
+                                      env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, cwd=ROOT))
+    outs = [p.communicate(timeout=600) for p in procs]
+    for p, (o, e) in zip(procs, outs):
+        assert p.returncode == 0, e[-2000:]
+    lines = [l for l in outs[0][0].splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["cpu_baseline"]["kind"] == "reference"
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
+    assert not [l for l in outs[1][0].splitlines() if l.startswith("{")]
