@@ -118,3 +118,13 @@ def test_partitioning_known_answers():
     for p, m in zip(parts, oracle.masks_of(allf, parts)):
         for i in p:
             assert oracle.subset_of(m, allf[i])
+
+
+def test_tile_shape_estimate_runs_small(capsys):
+    """The CPU tile-shape estimate runs on a small seeded table and reports
+    every tile shape it compares."""
+    from oracle import tile_shape_estimate
+    tile_shape_estimate.main(20000, 400, 2)
+    out = capsys.readouterr().out
+    for shape in ("32-filter tiles x1", "16-filter tiles x2", "8-filter tiles x4", "union of half selectors"):
+        assert shape in out
