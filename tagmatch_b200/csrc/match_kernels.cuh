@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                 if (lane >= (unsigned)o) incl += v;
             }
             const uint32_t n = __shfl_sync(kFull, incl, 7);
-            if (COUNT) w_cand += cnt;
+            if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
             if (n == 0) continue;
             uint32_t *list = s_list[warp];
             if (lane < 8) {
