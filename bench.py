@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--parity-samples", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-rates", default="200000,500000,1000000")
@@ -170,22 +172,57 @@ def shard_seed(rank):
     return SEED if rank == 0 else SEED + 7919 * rank
 
 
-def cpu_baseline(f, ko, k, q, seconds):
-    """The oracle's C port of test_matcher on all host cores, bounded sample."""
+def cpu_baseline(f, ko, k, q, seconds, unique=False):
+    """The oracle's C port of test_matcher on all host cores, bounded sample:
+    one scan of the table per query with its keys gathered (the work of
+    test_matcher.cc:74-81), reduced to a digest instead of printed."""
     from oracle import oracle
     cores = os.cpu_count() or 1
     n = max(cores, 8)
     t0 = time.perf_counter()
-    oracle.match(f, ko, k, q[:n], threads=cores)
+    oracle.match_digest(f, ko, k, q[:n], unique=unique, threads=cores)
     dt = time.perf_counter() - t0
     per_q = dt / n
     m = int(min(q.shape[0], max(n, seconds / max(per_q, 1e-9))))
     t0 = time.perf_counter()
-    oracle.match(f, ko, k, q[:m], threads=cores)
+    oracle.match_digest(f, ko, k, q[:m], unique=unique, threads=cores)
     dt = time.perf_counter() - t0
     return {"value": m / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {m} of the step's queries against the full {f.shape[0]}-filter table "
-                      f"(oracle/oracle.c restatement of test_matcher.cc:74-81), {dt:.1f} s"}
+            "sample": f"first {m} of the step's queries against the full {f.shape[0]}-filter table, one pass per "
+                      f"query (oracle/oracle.c restatement of test_matcher.cc:74-81), {dt:.1f} s"}
+
+
+def parity_check(tm, f, ko, k, q, base, B, unique, stream, samples):
+    """Checks the timed configuration itself: one more step with the same
+    tiles per work item and device batch; every (nq / samples)-th query's
+    keys are read back from the device and digested (count, multiset hash),
+    against the oracle's single-pass matcher on the same table."""
+    from oracle import oracle
+    from tagmatch_b200.tagmatch import read_device
+    nq = q.shape[0]
+    stride = max(1, nq // samples)
+    sel = np.arange(0, nq, stride)
+    got_c = np.zeros(sel.size, dtype=np.uint64)
+    got_h = np.zeros(sel.size, dtype=np.uint64)
+    j = 0
+    for b0 in range(0, nq, B):
+        n = min(B, nq - b0)
+        po, pk, _ = tm.match_batch_device(base + b0 * 24, n, unique=unique, stream=stream)
+        off = read_device(po, n + 1, np.uint64)
+        while j < sel.size and sel[j] < b0 + n:
+            i = int(sel[j]) - b0
+            keys = read_device(pk + int(off[i]) * 4, int(off[i + 1] - off[i]), np.uint32)
+            c, h = oracle.digest(np.array([0, keys.size], dtype=np.uint64), keys)
+            got_c[j], got_h[j] = c[0], h[0]
+            j += 1
+    t0 = time.perf_counter()
+    exp_c, exp_h = oracle.match_digest(f, ko, k, q[sel], unique=unique)
+    bad = int(np.count_nonzero((exp_c != got_c) | (exp_h != got_h)))
+    return {"checked": int(sel.size), "mismatches": bad, "every": int(stride),
+            "keys_checked": int(got_c.sum()), "oracle_s": round(time.perf_counter() - t0, 1),
+            "how": "per-query (count, multiset hash) of the device results of one more step at the timed "
+                   "configuration, against oracle/oracle.c's single-pass restatement of test_matcher.cc:74-81"
+                   + (" + tagmatch_query.hh:99-119 sort/unique" if unique else "")}
 
 
 def serving(args):
@@ -304,6 +341,12 @@ def run_ours(args):
                         "hit_records_per_query": round(st["records"] / max(st["queries"], 1), 2),
                         "keys_per_query": round(st["keys"] / max(st["queries"], 1), 2)}}
 
+    if tuned:
+        line["config"]["seg_tiles"] = tuned["seg_tiles"]
+    if rank == 0 and not args.no_parity:
+        line["parity"] = parity_check(tm, f, ko, k, q, base, B, args.unique, stream.cuda_stream, args.parity_samples)
+        line["parity"].update({"seg_tiles": tuned["seg_tiles"] if tuned else "engine default", "device_batch": B})
+
     # ---- end to end through the host C ABI ----
     if not args.no_e2e:
         tm.set_batch_limit(B)
@@ -353,7 +396,7 @@ def run_ours(args):
                        "keys_per_step": int(nk.value),
                        "api": "tm_match_batch (pinned host input and output buffers)"}
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(f, ko, k, q, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(f, ko, k, q, args.cpu_seconds, args.unique)
     if rank == 0 and world == 1 and not args.no_serve:
         line["serving"] = serving(args)
     if rank == 0:

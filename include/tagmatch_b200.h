@@ -114,9 +114,10 @@ int tm_set_batch_limit(tm_engine *e, uint32_t queries);
 int tm_match_batch(tm_engine *e, const uint32_t *queries, uint64_t n, int unique, uint64_t *out_offsets,
                    uint32_t *out_keys, uint64_t capacity, uint64_t *n_keys);
 
-/* Device-resident form on CUDA device 0: queries, results and stream are
- * device objects.  *d_offsets / *d_keys point into engine-owned device
- * memory valid until the next match call on this engine. */
+/* Device-resident form on the engine's first device (the CUDA device that
+ * was current at tm_create): queries, results and stream are device
+ * objects.  *d_offsets / *d_keys point into engine-owned device memory
+ * valid until the next match call on this engine. */
 int tm_match_batch_device(tm_engine *e, const uint32_t *d_queries, uint32_t n, int unique, const uint64_t **d_offsets,
                           const uint32_t **d_keys, uint64_t *n_keys, void *stream);
 
@@ -184,12 +185,19 @@ int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p
                              uint32_t *masks, uint32_t *sizes, uint64_t capacity, uint64_t *n_partitions);
 
 /* Autotuner (no reference counterpart): matches the n sample queries
- * [n][6] on device 0 with each candidate number of tiles per work item
+ * [n][6] on the engine's first device with each candidate number of tiles per work item
  * (32..8,192) and device batch size (8,192..262,144, at most n), timed with
  * CUDA events, and keeps the fastest for this engine.  Reports the chosen
  * values and the sample's queries/s.  Results do not depend on either. */
 int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch_limit,
                 double *queries_per_s);
+
+/* Tiles per work item of the subset test (what tm_autotune chooses;
+ * default 128): each work item is one 256-query chunk of a partition
+ * against this many of its tiles (up to 32 filters each).  No reference
+ * counterpart.  Results do not depend on it. */
+int tm_set_tiles_per_item(tm_engine *e, uint32_t seg_tiles);
+uint32_t tm_get_tiles_per_item(const tm_engine *e);
 
 /* Table statistics after consolidate. */
 typedef struct {

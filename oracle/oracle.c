@@ -136,6 +136,80 @@ int oracle_fill(const uint32_t *filters, uint64_t n, const uint32_t *key_off, co
 }
 
 /* ------------------------------------------------------------------ */
+/* Single pass per query with digests: the same work as test_matcher  */
+/* (test_matcher.cc:74-81: one scan of the table per query, the keys  */
+/* of every matching filter gathered), the keys reduced to a per-query */
+/* (count, multiset hash) instead of printed.  The hash of a key k is  */
+/* fin64(k + 0x9E3779B97F4A7C15) (the splitmix64 finalizer); a query's */
+/* hash is the wrapping sum over its keys, so it does not depend on    */
+/* key order.  unique != 0 sorts and de-duplicates first               */
+/* (tagmatch_query.hh:99-119).                                          */
+/* ------------------------------------------------------------------ */
+static inline uint64_t fin64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+typedef struct {
+    job_t j;
+    uint64_t *hashes;
+} digest_job_t;
+
+static void *digest_worker(void *arg) {
+    digest_job_t *d = (digest_job_t *)arg;
+    const job_t *j = &d->j;
+    size_t cap = 1 << 16;
+    uint32_t *buf = (uint32_t *)malloc(cap * sizeof(uint32_t));
+    for (uint64_t qi = j->q0; qi < j->q1; ++qi) {
+        const uint32_t *q = j->queries + qi * W;
+        uint64_t c = 0;
+        for (uint64_t f = 0; f < j->n; ++f) {
+            if (subset_of(j->filters + f * W, q)) {
+                uint32_t b = j->key_off[f], e = j->key_off[f + 1];
+                if (c + (e - b) > cap) {
+                    while (c + (e - b) > cap) cap *= 2;
+                    buf = (uint32_t *)realloc(buf, cap * sizeof(uint32_t));
+                }
+                memcpy(buf + c, j->keys + b, (size_t)(e - b) * sizeof(uint32_t));
+                c += e - b;
+            }
+        }
+        if (j->unique && c > 1) {
+            qsort(buf, (size_t)c, sizeof(uint32_t), cmp_u32);
+            uint64_t u = 1;
+            for (uint64_t k = 1; k < c; ++k) if (buf[k] != buf[u - 1]) buf[u++] = buf[k];
+            c = u;
+        }
+        uint64_t h = 0;
+        for (uint64_t k = 0; k < c; ++k) h += fin64((uint64_t)buf[k] + 0x9E3779B97F4A7C15ull);
+        j->counts[qi] = c;
+        d->hashes[qi] = h;
+    }
+    free(buf);
+    return NULL;
+}
+
+int oracle_match_digest(const uint32_t *filters, uint64_t n, const uint32_t *key_off, const uint32_t *keys,
+                        const uint32_t *queries, uint64_t nq, int unique, uint64_t *counts, uint64_t *hashes,
+                        int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if ((uint64_t)nthreads > nq) nthreads = nq ? (int)nq : 1;
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * nthreads);
+    digest_job_t *jobs = (digest_job_t *)malloc(sizeof(digest_job_t) * nthreads);
+    for (int t = 0; t < nthreads; ++t) {
+        job_t j = {filters, n, key_off, keys, queries, nq * t / nthreads, nq * (t + 1) / nthreads, unique, counts, NULL,
+                   NULL};
+        jobs[t].j = j;
+        jobs[t].hashes = hashes;
+        pthread_create(&th[t], NULL, digest_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    free(th); free(jobs);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Balanced partitioning, restated from partitioning.cc.               */
 /*                                                                     */
 /* The reference runs a thread pool over a queue of candidates         */

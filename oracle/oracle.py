@@ -41,6 +41,8 @@ def _load():
         lib.oracle_count.argtypes = [u32p, ctypes.c_uint64, u32p, u32p, u32p, ctypes.c_uint64, u64p, ctypes.c_int]
         lib.oracle_fill.argtypes = [u32p, ctypes.c_uint64, u32p, u32p, u32p, ctypes.c_uint64, ctypes.c_int, u64p, u32p,
                                     u64p, ctypes.c_int]
+        lib.oracle_match_digest.argtypes = [u32p, ctypes.c_uint64, u32p, u32p, u32p, ctypes.c_uint64, ctypes.c_int,
+                                            u64p, u64p, ctypes.c_int]
         lib.oracle_partition.restype = ctypes.c_int64
         lib.oracle_partition.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p, u32p, ctypes.c_uint64]
         lib.oracle_subset_of.argtypes = [u32p, u32p]
@@ -82,6 +84,25 @@ def match(filters, key_off, keys, queries, unique=False, threads=None):
     uo[1:] = np.cumsum(final[:nq])
     res = np.concatenate([out[int(offs[i]): int(offs[i]) + int(final[i])] for i in range(nq)]) if nq else out[:0]
     return uo, res.astype(np.uint32)
+
+
+def match_digest(filters, key_off, keys, queries, unique=False, threads=None):
+    """One scan of the table per query, as test_matcher.cc:74-81 does, with
+    each query's keys reduced to `digest`'s (count, multiset hash)."""
+    lib = _load()
+    threads = threads or os.cpu_count() or 1
+    f = np.ascontiguousarray(filters, dtype=np.uint32).reshape(-1, 6)
+    q = np.ascontiguousarray(queries, dtype=np.uint32).reshape(-1, 6)
+    ko = np.ascontiguousarray(key_off, dtype=np.uint32)
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    if k.size == 0:
+        k = np.zeros(1, dtype=np.uint32)
+    nq = q.shape[0]
+    counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    hashes = np.zeros(max(nq, 1), dtype=np.uint64)
+    lib.oracle_match_digest(_p32(f), f.shape[0], _p32(ko), _p32(k), _p32(q), nq, 1 if unique else 0, _p64(counts),
+                            _p64(hashes), threads)
+    return counts[:nq], hashes[:nq]
 
 
 def subset_of(f, q):

@@ -86,6 +86,8 @@ SIGNATURES = {
     "tm_balanced_partitioning": (ctypes.c_int, [u32p, ctypes.c_uint64, ctypes.c_uint32, u32p, u32p, u32p,
                                                 ctypes.c_uint64, u64p]),
     "tm_autotune": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_uint32, u32p, u32p, ctypes.POINTER(ctypes.c_double)]),
+    "tm_set_tiles_per_item": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "tm_get_tiles_per_item": (ctypes.c_uint32, [ctypes.c_void_p]),
     "tm_get_table_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableInfo)]),
     "tm_get_match_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MatchStats)]),
     "tm_reset_match_stats": (ctypes.c_int, [ctypes.c_void_p]),

@@ -94,8 +94,17 @@ def build_driver(quick=False):
     return DRIVER
 
 
+# Where the reference's sources are read from to build oracle/_ref (the
+# reference's own test_matcher and CPU partitioner); TAGMATCH_REF overrides.
+REFERENCE_SOURCES = "/root/reference"
+
+
 def build_oracle():
-    _run(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
+    ref = os.environ.get("TAGMATCH_REF") or (REFERENCE_SOURCES if os.path.isdir(REFERENCE_SOURCES) else "")
+    if ref:
+        cmd.append("REF=" + ref)
+    _run(cmd)
 
 
 def build_all(quick=False):

@@ -223,6 +223,13 @@ int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg
     return guard(e, [&] { e->eng.autotune(queries, n, seg_tiles, batch_limit, queries_per_s); });
 }
 
+int tm_set_tiles_per_item(tm_engine *e, uint32_t seg_tiles) {
+    if (!e) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.set_seg_tiles(seg_tiles); });
+}
+
+uint32_t tm_get_tiles_per_item(const tm_engine *e) { return e ? e->eng.seg_tiles() : 0; }
+
 int tm_get_table_info(tm_engine *e, tm_table_info *info) {
     if (!e || !info) return TM_ERR_INVALID;
     return guard(e, [&] {

@@ -485,7 +485,9 @@ void Engine::match_device_noalloc(const uint32_t *d_queries, uint32_t nq, bool u
         throw Error(TM_ERR_STATE, "no device table: call consolidate() first");
     Device &d = *devs_[0];
     TM_CUDA(cudaSetDevice(d.id));
-    match_batch_noalloc(d.table, d_queries, nq, unique, d_offsets, d_keys, capacity, n_keys, st ? st : d.stream);
+    if (!d.noalloc_scratch) d.noalloc_scratch = noalloc_scratch_address();
+    match_batch_noalloc(d.table, d_queries, nq, unique, seg_tiles_, d.noalloc_scratch, d_offsets, d_keys, capacity,
+                        n_keys, st ? st : d.stream);
 }
 
 void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, uint32_t *batch_out, double *qps_out) {
@@ -540,16 +542,26 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    seg_tiles_ = best_seg;
     batch_limit_ = best_batch;
-    for (auto &dv : devs_) {
-        dv->scratch.seg_tiles = best_seg;
-        for (auto &h : dv->host) h.scratch.seg_tiles = best_seg;
-        for (auto &ln : dv->lanes) ln.scratch.seg_tiles = best_seg;
-    }
+    apply_seg_tiles(best_seg);
     *seg_out = best_seg;
     *batch_out = best_batch;
     *qps_out = best;
+}
+
+void Engine::apply_seg_tiles(uint32_t seg) {
+    seg_tiles_ = seg;
+    for (auto &dv : devs_) {
+        dv->scratch.seg_tiles = seg;
+        for (auto &h : dv->host) h.scratch.seg_tiles = seg;
+        for (auto &ln : dv->lanes) ln.scratch.seg_tiles = seg;
+    }
+}
+
+void Engine::set_seg_tiles(uint32_t seg) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (seg == 0 || seg > (1u << 20)) throw Error(TM_ERR_INVALID, "tiles per work item must be in 1 .. 2^20");
+    apply_seg_tiles(seg);
 }
 
 void Engine::set_profiling(bool on) {

@@ -137,7 +137,7 @@ public:
     // through the exception when out_keys is too small (needed in *n_keys)
     void match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
                     uint64_t capacity, uint64_t *n_keys);
-    // synchronous batch match with device buffers on device 0
+    // synchronous batch match with device buffers on the first device
     void match_device(const uint32_t *d_queries, uint32_t nq, bool unique, const uint64_t **d_offsets,
                       const uint32_t **d_keys, uint64_t *n_keys, cudaStream_t st, BatchStats *bs, cudaEvent_t ev0,
                       cudaEvent_t ev1);
@@ -166,6 +166,9 @@ public:
     // sizes on a sample of queries (device timing, CUDA events) and keeps
     // the fastest; returns the chosen pair and its queries/s
     void autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch, double *qps);
+    // tiles per work item of the subset test (what autotune chooses)
+    void set_seg_tiles(uint32_t seg);
+    uint32_t seg_tiles() const { return seg_tiles_; }
     bool profiling() const { return profile_; }
     bool started() const { return started_; }
     // host copy of the consolidated filters (table order) and keys
@@ -208,9 +211,11 @@ private:
         MatchScratch scratch;
         bool table_ready = false;
         HostLane host[kHostLanes];  // synchronous host-buffer pipeline
+        void *noalloc_scratch = nullptr;  // device address of the no-allocation array (looked up once)
         Lane lanes[kLanes];         // asynchronous matcher lanes
     };
     void build_device_table(Device &d);
+    void apply_seg_tiles(uint32_t seg);
     Device &device(int i);
     void enqueue(RequestPtr r);
     void worker_loop(int dev, int lane);

@@ -69,8 +69,13 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
 // Narrows n keys (all < 65,536) to 16 bits into s.keys16 on stream st.
 const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s, cudaStream_t st);
 
-// The same pipeline with all scratch in a static device array (noalloc.cu).
-void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_out_offsets,
-                         uint32_t *d_out_keys, uint64_t capacity, uint64_t *n_keys, cudaStream_t st);
+// The same pipeline with all scratch in a static device array (noalloc.cu):
+// scratch is that array's device address on the current device, as
+// returned by noalloc_scratch_address().
+void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint32_t seg_tiles,
+                         void *scratch, uint64_t *d_out_offsets, uint32_t *d_out_keys, uint64_t capacity,
+                         uint64_t *n_keys, cudaStream_t st);
+// Device address of the no-allocation array on the current device.
+void *noalloc_scratch_address();
 
 }  // namespace tmb

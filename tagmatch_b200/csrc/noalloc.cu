@@ -25,13 +25,16 @@
 // calls on different streams that are not ordered -- race on the array.
 //
 // In host code the array's name is only a host-side stand-in, not a device
-// address.  The first call on a device looks up its device address with
-// cudaGetSymbolAddress (once per device, with that device current) and
-// caches it; make that first call before any stream capture.
+// address.  Each engine looks up the array's device address once per device
+// (cudaGetSymbolAddress, below, with that device current) at its first call
+// of this entry point, and keeps it with its device table; make that first
+// call before any stream capture.  A cudaDeviceReset frees the engine's
+// device table along with the module that holds the array, so after a reset
+// the engine is unusable anyway: create a new one, which looks the address
+// up again.
 #include "../../include/tagmatch_b200.h"
 #include "engine.cuh"
 #include "match_kernels.cuh"
-#include <mutex>
 #include <string>
 
 namespace tmb {
@@ -40,27 +43,19 @@ namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;  // 64 MiB per device
 constexpr uint32_t kNoAllocMaxQueries = 4096;
 constexpr uint32_t kNoAllocMaxPartitions = 16384;
-constexpr int kMaxDevices = 64;
-
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_setup_mtx;
-void *g_scratch_addr[kMaxDevices] = {};
+}  // namespace
 
-void *scratch_address() {
-    int dev = 0;
-    TM_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) throw Error(TM_ERR_INVALID, "device index out of range");
-    std::lock_guard<std::mutex> lk(g_setup_mtx);
-    if (!g_scratch_addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            throw Error(TM_ERR_CUDA, cuda_msg(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__));
-        g_scratch_addr[dev] = p;
-    }
-    return g_scratch_addr[dev];
+void *noalloc_scratch_address() {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        throw Error(TM_ERR_CUDA, cuda_msg(e, "cudaGetSymbolAddress(g_noalloc_scratch)", __FILE__, __LINE__));
+    return p;
 }
+
+namespace {
 
 // Bump carving of the static array, 256-byte aligned pieces.
 struct Arena {
@@ -85,13 +80,14 @@ struct Arena {
 
 // Work-plan counts per partition: 256-query chunks, and chunks x tile segments.
 __global__ void k_plan_counts(const uint32_t *__restrict__ part_count, const uint32_t *__restrict__ part_tile_begin,
-                              uint32_t n_parts, uint32_t *__restrict__ nchunks, uint32_t *__restrict__ nitems) {
+                              uint32_t n_parts, uint32_t seg_tiles, uint32_t *__restrict__ nchunks,
+                              uint32_t *__restrict__ nitems) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_parts) return;
     const uint32_t c = (part_count[p] + kChunk - 1) / kChunk;
     const uint32_t nt = part_tile_begin[p + 1] - part_tile_begin[p];
     nchunks[p] = c;
-    nitems[p] = c * ((nt + kSegTiles - 1) / kSegTiles);
+    nitems[p] = c * ((nt + seg_tiles - 1) / seg_tiles);
 }
 
 // Exclusive scan with block sums held in the arena (up to 2048 x 2048 elements).
@@ -116,8 +112,9 @@ void scan_fixed(const Tin *in, Tout *out, size_t n, uint64_t *sums, uint64_t *of
 
 // The whole pipeline over the static array.  d_out_offsets: n + 1 entries;
 // d_out_keys: capacity keys; both device memory owned by the caller.
-void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint64_t *d_out_offsets,
-                         uint32_t *d_out_keys, uint64_t capacity, uint64_t *n_keys, cudaStream_t st) {
+void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool unique, uint32_t seg_tiles,
+                         void *scratch, uint64_t *d_out_offsets, uint32_t *d_out_keys, uint64_t capacity,
+                         uint64_t *n_keys, cudaStream_t st) {
     if (nq > kNoAllocMaxQueries)
         throw Error(TM_ERR_INVALID, "tm_match_batch_device_noalloc: at most " + std::to_string(kNoAllocMaxQueries) +
                                         " queries per call, got " + std::to_string(nq));
@@ -128,7 +125,8 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     int dev = 0, sms = 0;
     TM_CUDA(cudaGetDevice(&dev));
     TM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    Arena ar{static_cast<unsigned char *>(scratch_address())};
+    if (seg_tiles == 0) throw Error(TM_ERR_INVALID, "tiles per work item must be positive");
+    Arena ar{static_cast<unsigned char *>(scratch)};
     *n_keys = 0;
     if (nq == 0 || P == 0 || t.n_tiles == 0) {
         TM_CUDA(cudaMemsetAsync(d_out_offsets, 0, (size_t(nq) + 1) * sizeof(uint64_t), st));
@@ -165,7 +163,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         TM_CHECK_LAUNCH();
     }
     scan_fixed<uint32_t, uint32_t>(part_count, part_off, P, sums, offs, st);
-    k_plan_counts<<<blocks_for(P, 256), 256, 0, st>>>(part_count, t.part_tile_begin.p, P, nchunks, nitems);
+    k_plan_counts<<<blocks_for(P, 256), 256, 0, st>>>(part_count, t.part_tile_begin.p, P, seg_tiles, nchunks, nitems);
     TM_CHECK_LAUNCH();
     scan_fixed<uint32_t, uint32_t>(nchunks, chunk_off, P, sums, offs, st);
     scan_fixed<uint32_t, uint32_t>(nitems, item_off, P, sums, offs, st);
@@ -193,7 +191,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     if (rec_room < 256) throw Error(TM_ERR_CAPACITY, "no-allocation scratch exhausted before the hit records; split the batch");
     HitRec *recs = ar.take<HitRec>(rec_room - 32, "hit records");
     MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, part_count, part_off, item_off, chunk_off, queue, slices,
-                P, uint32_t(kSegTiles), counters, recs, (unsigned long long)(rec_room - 32), nullptr};
+                P, seg_tiles, counters, recs, (unsigned long long)(rec_room - 32), nullptr};
     k_match<false><<<unsigned(sms) * 4, kMatchThreads, 0, st>>>(a);
     TM_CHECK_LAUNCH();
     unsigned long long hc[3] = {0, 0, 0};

@@ -247,6 +247,13 @@ class TagMatch:
                                           ctypes.byref(qps)))
         return seg.value, bl.value, qps.value
 
+    def set_tiles_per_item(self, seg_tiles):
+        """Tiles per work item of the subset test (the autotuner's knob)."""
+        self._check(self._lib.tm_set_tiles_per_item(self._h, seg_tiles))
+
+    def get_tiles_per_item(self):
+        return self._lib.tm_get_tiles_per_item(self._h)
+
     def set_profiling(self, on):
         self._check(self._lib.tm_set_profiling(self._h, 1 if on else 0))
 
@@ -266,6 +273,37 @@ class TagMatch:
         st = _native.MatchStats()
         self._check(self._lib.tm_get_match_stats(self._h, ctypes.byref(st)))
         return {k: getattr(st, k) for k, _ in st._fields_}
+
+
+_cudart_lib = None
+
+
+def _cudart():
+    global _cudart_lib
+    if _cudart_lib is None:
+        import glob
+        names = ["libcudart.so.12", "libcudart.so"] + sorted(glob.glob("/usr/local/cuda*/lib64/libcudart.so*"))
+        for name in names:
+            try:
+                _cudart_lib = ctypes.CDLL(name)
+                break
+            except OSError:
+                continue
+        else:
+            raise OSError("libcudart not found")
+    return _cudart_lib
+
+
+def read_device(ptr, count, dtype):
+    """Copies count elements of dtype from device address ptr (as returned by
+    match_batch_device) into a new numpy array (synchronous cudaMemcpy)."""
+    out = np.empty(int(count), dtype=dtype)
+    if out.size:
+        st = _cudart().cudaMemcpy(ctypes.c_void_p(out.ctypes.data), ctypes.c_void_p(ptr), ctypes.c_size_t(out.nbytes),
+                                  2)
+        if st != 0:
+            raise TagMatchError(_native.TM_ERR_CUDA, f"cudaMemcpy device->host failed ({st})")
+    return out
 
 
 def balanced_partitioning(filters, max_p):

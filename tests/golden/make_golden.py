@@ -54,10 +54,13 @@ def parse_test_io(src):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("TAGMATCH_REF"),
+                    help="reference source tree (default: $TAGMATCH_REF)")
     ap.add_argument("--skip-config0", action="store_true")
     args = ap.parse_args()
     ref = args.reference
+    if not ref:
+        raise SystemExit("give the reference source tree with --reference or TAGMATCH_REF")
     if not oracle.have_ref():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle REF=...` first")
 

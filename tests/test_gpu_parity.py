@@ -272,6 +272,40 @@ def test_config1_table_sampled_parity():
     tm.close()
 
 
+@pytest.mark.parametrize("seg_tiles", [2048, 8192])
+def test_config1_large_work_items_device_batch(seg_tiles):
+    """The shapes the bench times after autotuning: the 10M-filter table,
+    one device batch of 131,072 queries, 2,048 or 8,192 tiles per work item.
+    Every 655th query's keys are read back from the device and compared, as
+    (count, multiset hash), with the oracle's single pass over the table."""
+    import torch
+    from tagmatch_b200.tagmatch import read_device
+    f, ko, k, q = workload.config("config1", n_queries=131072)
+    tm = engine_with(f, ko, k, 65536)
+    tm.set_tiles_per_item(seg_tiles)
+    assert tm.get_tiles_per_item() == seg_tiles
+    dq = torch.from_numpy(q.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    sel = np.arange(0, q.shape[0], 655)
+    exp = {u: oracle.match_digest(f, ko, k, q[sel], unique=u) for u in (False, True)}
+    for unique in (False, True):
+        po, pk, nk = tm.match_batch_device(dq.data_ptr(), q.shape[0], unique=unique)
+        off = read_device(po, q.shape[0] + 1, np.uint64)
+        assert int(off[-1]) == nk
+        assert np.all(off[1:] >= off[:-1])
+        got_c, got_h = [], []
+        for i in sel:
+            keys = read_device(pk + int(off[i]) * 4, int(off[i + 1] - off[i]), np.uint32)
+            if unique:
+                assert np.all(keys[1:] > keys[:-1])
+            c, h = oracle.digest(np.array([0, keys.size], dtype=np.uint64), keys)
+            got_c.append(c[0])
+            got_h.append(h[0])
+        assert np.array_equal(np.array(got_c, dtype=np.uint64), exp[unique][0])
+        assert np.array_equal(np.array(got_h, dtype=np.uint64), exp[unique][1])
+    tm.close()
+
+
 @pytest.mark.parametrize("mode", [_native.TM_FLUSH_IMMEDIATE, _native.TM_FLUSH_SINGLE, _native.TM_FLUSH_FULL_OR_LATENCY])
 def test_submit_requests_same_alone_and_mixed(mode):
     """Serving: requests of 1..700 queries, merged into shared device batches
@@ -434,7 +468,8 @@ def test_autotune_keeps_results():
     tm = engine_with(f, ko, k, 8192)
     off0, keys0 = tm.match_batch(q)
     seg, batch, qps = tm.autotune(q)
-    assert seg in (32, 64, 128, 256, 512) and batch in (8192, 16384, 20000) and qps > 0
+    assert seg in tuple(32 << i for i in range(9)) and batch in (8192, 16384, 20000) and qps > 0
+    assert tm.get_tiles_per_item() == seg
     off1, keys1 = tm.match_batch(q)
     assert_same_multisets(off0, keys0, off1, keys1)
     tm.close()
