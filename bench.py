@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--batch", type=int, default=131072, help="queries per device batch")
     ap.add_argument("--unique", action="store_true", help="time match_unique instead of match")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--seg-tiles", type=int, default=0, help="tiles per work item (instead of autotuning)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
@@ -264,7 +265,9 @@ def run_ours(args):
     nq = q.shape[0]
     B = args.batch
     tuned = None
-    if not args.no_autotune:
+    if args.seg_tiles:
+        tm.set_tiles_per_item(args.seg_tiles)
+    elif not args.no_autotune:
         # tiles per work item and device batch size, timed on a sample
         seg, bl, tqps = tm.autotune(q[: min(nq, 262144)])
         B = bl
@@ -341,11 +344,10 @@ def run_ours(args):
                         "hit_records_per_query": round(st["records"] / max(st["queries"], 1), 2),
                         "keys_per_query": round(st["keys"] / max(st["queries"], 1), 2)}}
 
-    if tuned:
-        line["config"]["seg_tiles"] = tuned["seg_tiles"]
+    line["config"]["seg_tiles"] = tm.get_tiles_per_item()
     if rank == 0 and not args.no_parity:
         line["parity"] = parity_check(tm, f, ko, k, q, base, B, args.unique, stream.cuda_stream, args.parity_samples)
-        line["parity"].update({"seg_tiles": tuned["seg_tiles"] if tuned else "engine default", "device_batch": B})
+        line["parity"].update({"seg_tiles": tm.get_tiles_per_item(), "device_batch": B})
 
     # ---- end to end through the host C ABI ----
     if not args.no_e2e:

@@ -25,18 +25,20 @@
 //                bulk TMA copies (cp.async.bulk + mbarrier), double-buffered:
 //                the next item loads while this one is matched, and the
 //                buffer is released by per-warp mbarrier arrivals instead of
-//                a CTA barrier.  Each warp takes one tile of <= 32 filters in
-//                registers; the tile's AND mask selects candidate queries by
-//                OR-ing the slices of its bits (8 lanes, one 32-query word
-//                each); each candidate is tested against the 32 filters with
-//                6 LOP3s; a ballot per candidate gives the tile's hit mask
-//                for that query, staged as a (query, tile, mask) record in a
-//                per-warp shared-memory buffer flushed with one global atomic;
-//   k_key_count  per record: its key total (a run of adjacent hit bits is
-//                one key range of the tile's slots), added to the query's;
+//                a CTA barrier.  Each warp takes one tile of <= 32 filters;
+//                the tile's AND mask selects candidate queries by OR-ing the
+//                slices of its bits (8 lanes, one 32-query word each); the
+//                candidates are tested either one per lane against the
+//                tile's filters broadcast from shared memory, or, when they
+//                are few, four at a time against the tile held one filter
+//                per lane (6 LOP3s per (query, filter) either way); each
+//                (query, tile) with a hit becomes a (query, tile, hit mask,
+//                key count) record, staged per warp in shared memory and
+//                flushed with one global atomic, and its key count is added
+//                to the query's total;
 //   k_key_fill   after a prefix sum of the query totals: one cursor atomic
-//                per group of same-query records in a warp, then one
-//                contiguous key range per run of hit bits;
+//                per record, then one contiguous key range per run of hit
+//                bits, four records per lane in flight;
 //   k_unique_*   match_unique: per-query bitmap (small key spaces, output
 //                comes out sorted) or per-query block radix sort + unique.
 // Result overflow is exact: the record buffer is regrown and the batch re-run
@@ -81,6 +83,17 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     ev_end = o.ev_end;
     o.ev_begin = o.ev_end = nullptr;
     return *this;
+}
+
+// Estimated cost of one 4-candidate trip of the subset test's
+// lane-per-filter loop, against which the lane-per-query pass is weighed
+// for each tile (TM_FPL_TRIP_COST overrides it; results do not depend on it).
+uint32_t fpl_trip_cost() {
+    static const uint32_t v = [] {
+        const char *e = std::getenv("TM_FPL_TRIP_COST");
+        return e ? uint32_t(std::strtoul(e, nullptr, 10)) : 60u;
+    }();
+    return v;
 }
 
 const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s, cudaStream_t st) {
@@ -203,9 +216,12 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             s.work.reserve(8);
             TM_CUDA(cudaMemsetAsync(s.work.p, 0, 8 * sizeof(unsigned long long), st));
         }
-        MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, s.part_count.p, s.part_off.p, s.item_off.p,
-                    s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p, s.recs.p,
-                    (unsigned long long)s.recs.cap, work_counters ? s.work.p : nullptr};
+        // per-query key totals are summed by the subset test itself
+        TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
+        MatchArgs a{t.tile_words.p, t.tile_info.p, t.tile_keys.p, t.slot_key_off.p, t.part_tile_begin.p, s.part_count.p,
+                    s.part_off.p, s.item_off.p, s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p,
+                    s.recs.p, (unsigned long long)s.recs.cap, s.qkeys.p, fpl_trip_cost(),
+                    work_counters ? s.work.p : nullptr};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
             if (!s.ev_begin) {
@@ -214,8 +230,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             }
             TM_CUDA(cudaEventRecord(s.ev_begin, st));
         }
-        if (work_counters) k_match<true><<<unsigned(s.sm_count) * 4, kMatchThreads, 0, st>>>(a);
-        else k_match<false><<<unsigned(s.sm_count) * 4, kMatchThreads, 0, st>>>(a);
+        if (work_counters) launch_match<true>(a, unsigned(s.sm_count) * 4, st);
+        else launch_match<false>(a, unsigned(s.sm_count) * 4, st);
         TM_CHECK_LAUNCH();
         if (s.profile) TM_CUDA(cudaEventRecord(s.ev_end, st));
         if (match_end) TM_CUDA(cudaEventRecord(match_end, st));
@@ -225,9 +241,9 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             unsigned long long w[8];
             TM_CUDA(cudaMemcpy(w, s.work.p, sizeof(w), cudaMemcpyDeviceToHost));
             std::fprintf(stderr,
-                         "[tm work] queries %u tile_visits %llu and_bits %llu candidates %llu trips %llu items %llu "
-                         "records %llu\n",
-                         nq, w[0], w[1], w[2], w[3], w[4], hc[1]);
+                         "[tm work] queries %u tile_visits %llu query_passes %llu candidates %llu filter_trips %llu "
+                         "items %llu query_groups %llu records %llu pairs %llu\n",
+                         nq, w[0], w[1], w[2], w[3], w[4], w[5], hc[1], hc[3]);
         }
         if (s.profile) {
             float ms = 0.f;
@@ -242,19 +258,13 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     }
     bs.records = hc[1];
     // ---- keys ----
-    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256), unsigned(s.sm_count) * 16));
-    // record-count readback, count, fill, key-total readback; each retry: match + readback
-    bs.launches += 4 + scan_launches(nq) + 2 * uint32_t(bs.retries);
-    TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
-    k_key_count<<<gblocks, 256, 0, st>>>(s.recs.p, s.counters.p, t.slot_key_off.p, s.qkeys.p);
-    TM_CHECK_LAUNCH();
+    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256 * kFillPerLane), unsigned(s.sm_count) * 16));
+    // record-count readback, fill, key-total readback; each retry: match + readback
+    bs.launches += 3 + scan_launches(nq) + 2 * uint32_t(bs.retries);
     exclusive_scan<uint32_t, uint64_t>(s.qkeys.p, s.qoff.p, nq, s.scr, st);
-    // key total and matching pairs (k_key_count's count in counters[3])
-    uint64_t total = 0, pairs = 0;
-    const uint32_t *tb = read_back(s, s.qoff.p + nq, 2, s.counters.p + 3, 2, st);
-    std::memcpy(&total, tb, sizeof(uint64_t));
-    std::memcpy(&pairs, tb + 2, sizeof(uint64_t));
-    bs.pairs = pairs;
+    uint64_t total = 0;
+    std::memcpy(&total, read_back(s, s.qoff.p + nq, 2, nullptr, 0, st), sizeof(uint64_t));
+    bs.pairs = hc[3];
     s.keys.reserve(std::max<uint64_t>(total, 1));
     s.qcursor.reserve(nq);
     TM_CUDA(cudaMemsetAsync(s.qcursor.p, 0, nq * sizeof(uint32_t), st));

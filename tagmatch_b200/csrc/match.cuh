@@ -66,6 +66,9 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
                  const uint64_t **d_offsets, const uint32_t **d_keys, uint64_t *n_keys, BatchStats *stats,
                  cudaStream_t st, cudaEvent_t match_begin = nullptr, cudaEvent_t match_end = nullptr);
 
+// The subset test's path-choice constant (see match.cu).
+uint32_t fpl_trip_cost();
+
 // Narrows n keys (all < 65,536) to 16 bits into s.keys16 on stream st.
 const uint16_t *narrow_keys(const uint32_t *d_keys, uint64_t n, MatchScratch &s, cudaStream_t st);
 

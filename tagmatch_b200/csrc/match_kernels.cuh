@@ -142,9 +142,49 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, uint32_
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Bounded wait on an mbarrier phase; false when the limit expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    unsigned long long spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++spins > kSpinLimit) return false;
+    }
+    return true;
+}
+
+// Keys of the filters in a hit mask.  The table keeps keys in slot order, so
+// a run of adjacent set bits [lo, hi) is the one key range [o[lo], o[hi])
+// (o: the tile's slot key offsets, 33 of them).  Calls f(begin, end) per run.
+template <class F>
+__device__ __forceinline__ void for_each_key_run(const uint32_t *__restrict__ o, uint32_t mask, F f) {
+    uint64_t m = mask;
+    while (m) {
+        const int lo = __ffsll(m) - 1;
+        const uint64_t filled = m + (1ull << lo);  // the carry clears the run and sets bit hi
+        const int hi = __ffsll(filled & ~m) - 1;
+        f(o[lo], o[hi]);
+        m &= filled;
+    }
+}
+
+// Keys of hit mask m of tile t: from the tile's key-count bit planes, or,
+// when m touches a filter with 8 keys or more, from the slot offsets.
+__device__ __forceinline__ uint32_t mask_keys(const TileKeys &tk, uint32_t m, const uint32_t *__restrict__ slot_key_off,
+                                              uint32_t t) {
+    if (!(m & tk.wide)) return keys_of_mask(tk, m);
+    uint32_t nk = 0;
+    for_each_key_run(slot_key_off + size_t(t) * kTile, m, [&](uint32_t b, uint32_t e) { nk += e - b; });
+    return nk;
+}
+
 struct MatchArgs {
     const uint32_t *tile_words;
     const TileInfo *tile_info;
+    const TileKeys *tile_keys;
+    const uint32_t *slot_key_off;
     const uint32_t *part_tile_begin;
     const uint32_t *part_count;
     const uint32_t *part_off;
@@ -159,9 +199,12 @@ struct MatchArgs {
     unsigned long long *counters;
     HitRec *recs;
     unsigned long long rec_cap;
-    // optional work counters (diagnostics): [0] tile visits, [1] AND-mask
-    // bits OR-ed, [2] candidate (query, tile) pairs, [3] candidate loop
-    // trips, [4] items; null when off
+    uint32_t *qkeys;               // [batch queries] key totals, zeroed by the caller
+    uint32_t fpl_trip_cost;        // path choice: estimated cost of one 4-candidate trip of the lane-per-filter loop
+    // optional work counters (diagnostics): [0] tile visits, [1] passes of
+    // the lane-per-query path, [2] candidate (query, tile) pairs, [3] trips
+    // of the lane-per-filter path, [4] items, [5] 4-filter groups tested by
+    // the lane-per-query path; null when off
     unsigned long long *work;
 };
 
@@ -176,6 +219,20 @@ struct __align__(128) Stage {
     uint32_t z[kSliceWords];                 // 6 KB
 };
 
+// Shared memory of one matcher CTA (dynamic; ~51 KB, 4 CTAs per SM).
+struct MatchSmem {
+    Stage st[2];
+    HitRec rec[kMatchWarps][kWarpRecs];                  // staged hit records per warp
+    uint32_t list[kMatchWarps][kChunk + 8];              // candidate lists per warp
+    uint4 tf[kMatchWarps][kWords][kTile / 4];            // a warp's tile: word k of filters 4 g .. 4 g + 3
+    uint64_t full[2], empty[2];
+    uint32_t item[2];
+    int fail;
+    // thread 0's record of the copies in flight (bit s: stage s), with the
+    // parity of the phase that completes each
+    uint32_t inflight, inflight_par;
+};
+
 // Moves a warp's n staged records to the global record buffer (one atomic
 // reserves their place; past the capacity they are only counted, and the
 // host re-runs the batch with a larger buffer).
@@ -188,19 +245,6 @@ __device__ __forceinline__ void flush_recs(HitRec *buf, uint32_t n, const MatchA
         for (uint32_t i = lane; i < n; i += 32) a.recs[base + i] = buf[i];
     }
     __syncwarp();
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// Bounded wait on an mbarrier phase; false when the limit expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    unsigned long long spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if (++spins > kSpinLimit) return false;
-    }
-    return true;
 }
 
 struct ItemRef {
@@ -230,275 +274,387 @@ __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
 
 // Thread 0: claim the next item and start its copy into stage `buf`; the
 // item id is published through the full barrier's phase completion.
-__device__ __forceinline__ void produce(const MatchArgs &a, uint32_t total, Stage *st, uint64_t *full, uint32_t *s_item,
-                                        int buf) {
+// Returns whether a copy is in flight.
+__device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, MatchSmem &S, int buf) {
     const uint32_t item = uint32_t(atomicAdd(&a.counters[0], 1ull));
-    s_item[buf] = item;
+    S.item[buf] = item;
     if (item < total) {
         const ItemRef r = locate(a, item);
         const uint32_t qbytes = r.nq * kQueueWords * sizeof(uint32_t);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&full[buf], qbytes + kSliceWords * sizeof(uint32_t));
-        tma_bulk_g2s(st[buf].q, a.queue + size_t(r.qbase) * kQueueWords, qbytes, &full[buf]);
-        tma_bulk_g2s(st[buf].z, a.slices + size_t(r.zchunk) * kSliceWords, kSliceWords * sizeof(uint32_t), &full[buf]);
-    } else {
-        mbar_arrive(&full[buf]);  // nothing to copy: complete the phase so consumers see the end
+        mbar_expect_tx(&S.full[buf], qbytes + kSliceWords * sizeof(uint32_t));
+        tma_bulk_g2s(S.st[buf].q, a.queue + size_t(r.qbase) * kQueueWords, qbytes, &S.full[buf]);
+        tma_bulk_g2s(S.st[buf].z, a.slices + size_t(r.zchunk) * kSliceWords, kSliceWords * sizeof(uint32_t), &S.full[buf]);
+        return true;
     }
+    mbar_arrive(&S.full[buf]);  // nothing to copy: complete the phase so consumers see the end
+    return false;
 }
 
-// COUNT: diagnostics instantiation that also tallies its work (a.work).
+// The subset test.  Persistent CTAs take work items (partition, 256-query
+// chunk, segment of the partition's tiles) from an atomic counter; thread 0
+// stages each item's query records and slices with bulk TMA copies into one
+// of two buffers while the CTA matches the other.  Each warp takes one tile
+// (<= 32 filters) at a time:
+//  * selection: the tile's 8 selector bits (bits every member holds); lanes
+//    0-7 OR the "lacks bit" slices of their 32-query word, so a query that
+//    lacks any of them is dropped; the remaining candidates are written to
+//    the warp's list (lane l compacts byte l & 3 of word l >> 2);
+//  * many candidates: one candidate query per lane, the tile's filters read
+//    from shared memory (one broadcast 128-bit load gives word k of four
+//    filters): 6 LOP3 per (query, filter), the lane's hit mask over the tile
+//    built bit by bit; one pass per 32 candidates;
+//  * few candidates: one filter per lane (the tile in registers), four
+//    candidates per trip, one ballot per candidate for its hit mask;
+//  * each (query, tile) with a hit becomes a 16-byte record (query, tile,
+//    hit mask, key count from the tile's key-count bit planes), staged in a
+//    per-warp buffer and flushed with one atomic; the query's key total is
+//    added to qkeys[query] (for the prefix sum that places its keys).
+// The path per tile is chosen from the candidate count and the tile size
+// (estimated instruction costs; the choice does not change results).
 template <bool COUNT>
 __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4 CTAs per SM: up to 64 registers
-    __shared__ Stage st[2];
-    __shared__ __align__(16) HitRec s_rec[kMatchWarps][kWarpRecs];
-    __shared__ __align__(16) uint32_t s_list[kMatchWarps][kChunk + 4];  // per-warp candidate lists
-    __shared__ __align__(8) uint64_t full[2], empty[2];
-    __shared__ uint32_t s_item[2];
-    __shared__ int s_fail;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MatchSmem &S = *reinterpret_cast<MatchSmem *>(smem_raw);
     const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t total = a.item_off[a.n_parts];
     if (tid < 2 * kQueueWords) {
         const uint32_t k = tid % kQueueWords;
-        st[tid / kQueueWords].q[kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
+        S.st[tid / kQueueWords].q[kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
     }
     if (tid == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init(&empty[0], kMatchWarps);
-        mbar_init(&empty[1], kMatchWarps);
+        mbar_init(&S.full[0], 1);
+        mbar_init(&S.full[1], 1);
+        mbar_init(&S.empty[0], kMatchWarps);
+        mbar_init(&S.empty[1], kMatchWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_fail = 0;
+        S.fail = 0;
     }
     __syncthreads();
-    if (tid == 0) produce(a, total, st, full, s_item, 0);
-    uint32_t w_tiles = 0, w_bits = 0, w_cand = 0, w_trips = 0, w_items = 0;
-    uint32_t wn = 0;  // records staged by this warp (warp-uniform)
+    // thread 0 keeps track of the copies in flight (stage, wait parity), so
+    // that no copy still targets this CTA's shared memory when it exits
+    if (tid == 0) {
+        S.inflight = produce(a, total, S, 0) ? 1u : 0u;
+        S.inflight_par = 0;
+    }
+    uint32_t w_tiles = 0, w_passes = 0, w_cand = 0, w_trips = 0, w_items = 0, w_groups = 0;
+    uint32_t wn = 0;     // records staged by this warp (warp-uniform)
+    uint32_t pairs = 0;  // matching (query, filter) pairs found by this lane
     const uint32_t lane_lt = (1u << lane) - 1u;
+    uint32_t *list = S.list[warp];
+    uint32_t *tfw = reinterpret_cast<uint32_t *>(S.tf[warp]);
     for (uint32_t it = 0;; ++it) {
         const int b = it & 1;
         // prefetch the next item into the other stage once every warp has
         // released it (it held item it - 1)
         if (tid == 0) {
             bool ok = true;
-            if (it >= 1) ok = mbar_wait(&empty[b ^ 1], ((it - 1) >> 1) & 1);
-            if (ok) produce(a, total, st, full, s_item, b ^ 1);
-            else { atomicOr(&a.counters[2], 1ull); s_fail = 1; }
+            if (it >= 1) ok = mbar_wait(&S.empty[b ^ 1], ((it - 1) >> 1) & 1);
+            if (ok) {
+                const uint32_t bit = 1u << (b ^ 1);
+                S.inflight = produce(a, total, S, b ^ 1) ? S.inflight | bit : S.inflight & ~bit;
+                S.inflight_par = ((it + 1) >> 1) & 1 ? S.inflight_par | bit : S.inflight_par & ~bit;
+            } else {
+                atomicOr(&a.counters[2], 1ull);
+                S.fail = 1;
+            }
         }
         // every exit is taken by whole warps (record flushes use the full warp)
-        const bool got = mbar_wait(&full[b], (it >> 1) & 1);
+        const bool got = mbar_wait(&S.full[b], (it >> 1) & 1);
+        if (tid == 0 && got) S.inflight &= ~(1u << b);
         if (!__all_sync(kFull, got)) {
             if (lane == 0) atomicOr(&a.counters[2], 2ull);
             break;
         }
-        const uint32_t item = s_item[b];
-        if (__any_sync(kFull, item >= total || s_fail)) break;
+        const uint32_t item = S.item[b];
+        if (__any_sync(kFull, item >= total || S.fail)) break;
         const ItemRef r = locate(a, item);
         if (COUNT) ++w_items;
-        const uint4 *sq = reinterpret_cast<const uint4 *>(st[b].q);
-        const uint32_t *sz = st[b].z;
+        const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[b].q);
+        const uint32_t *sz = S.st[b].z;
         for (uint32_t t = r.tb + warp; t < r.te; t += kMatchWarps) {
+            const TileInfo ti = a.tile_info[t];
             uint32_t f[kWords];
 #pragma unroll
             for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
-            const TileInfo ti = a.tile_info[t];
-            const bool lane_valid = lane < ti.count;
-            const uint32_t vm = ti.count >= 32u ? kFull : (1u << ti.count) - 1u;  // lanes holding a filter
             if (COUNT) ++w_tiles;
             // candidates: queries holding the tile's selection bits; lane
             // w < 8 ORs the "lacks" slices for queries 32 w .. 32 w + 31
-            uint32_t lack = 0;
+            uint32_t cand_word = 0;
             if (lane < 8) {
                 const uint32_t *zl = sz + lane;
-                lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
-                       zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] | zl[(ti.sel[1] & 0xFFu) * 8] |
-                       zl[((ti.sel[1] >> 8) & 0xFFu) * 8] | zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
+                const uint32_t lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
+                                      zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] |
+                                      zl[(ti.sel[1] & 0xFFu) * 8] | zl[((ti.sel[1] >> 8) & 0xFFu) * 8] |
+                                      zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
+                cand_word = ~lack;
+                if (lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
             }
-            if (COUNT) w_bits += kSelBits;
-            uint32_t cand_word = lane < 8 ? ~lack : 0u;
-            if (lane < 8 && lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
             // compact candidate list (uint4 index of each query record):
-            // lanes 0-7 write the queries of their 32-query word in order
-            const uint32_t cnt = __popc(cand_word);
+            // lane l writes the candidates of byte l & 3 of word l >> 2
+            const uint32_t cw = __shfl_sync(kFull, cand_word, lane >> 2);
+            uint32_t byte = (cw >> ((lane & 3) * 8)) & 0xFFu;
+            const uint32_t cnt = __popc(byte);
             uint32_t incl = cnt;
 #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
+            for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t v = __shfl_up_sync(kFull, incl, o);
                 if (lane >= (unsigned)o) incl += v;
             }
-            const uint32_t n = __shfl_sync(kFull, incl, 7);
+            const uint32_t n = __shfl_sync(kFull, incl, 31);
             if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
             if (n == 0) continue;
-            uint32_t *list = s_list[warp];
-            if (lane < 8) {
-                uint32_t pos = incl - cnt, c = cand_word;
-                while (c) {
-                    list[pos++] = (lane * 32 + __ffs(c) - 1) * 2;
-                    c &= c - 1;
+            {
+                uint32_t pos = incl - cnt;
+                const uint32_t q0 = (lane >> 2) * 32 + (lane & 3) * 8;
+                while (byte) {
+                    list[pos++] = (q0 + __ffs(byte) - 1) * 2;
+                    byte &= byte - 1;
                 }
-            } else if (lane < 12) {
-                list[n + lane - 8] = kChunk * 2;  // pad to a multiple of 4: the stage's pad record
+                if (lane < 4) list[n + lane] = kChunk * 2;  // pad to a multiple of 4: the stage's pad record
             }
-            __syncwarp();
-            for (uint32_t i = 0; i < n; i += 4) {
-                if (COUNT) ++w_trips;
-                const uint4 idx = *reinterpret_cast<const uint4 *>(&list[i]);
-                const uint4 p0 = sq[idx.x], p1 = sq[idx.x + 1];
-                const uint4 q0 = sq[idx.y], q1 = sq[idx.y + 1];
-                const uint4 r0 = sq[idx.z], r1 = sq[idx.z + 1];
-                const uint4 u0 = sq[idx.w], u1 = sq[idx.w + 1];
-                uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
-                x0 = andnot_or(f[1], p0.y, x0);
-                x1 = andnot_or(f[1], q0.y, x1);
-                x2 = andnot_or(f[1], r0.y, x2);
-                x3 = andnot_or(f[1], u0.y, x3);
-                x0 = andnot_or(f[2], p0.z, x0);
-                x1 = andnot_or(f[2], q0.z, x1);
-                x2 = andnot_or(f[2], r0.z, x2);
-                x3 = andnot_or(f[2], u0.z, x3);
-                x0 = andnot_or(f[3], p0.w, x0);
-                x1 = andnot_or(f[3], q0.w, x1);
-                x2 = andnot_or(f[3], r0.w, x2);
-                x3 = andnot_or(f[3], u0.w, x3);
-                x0 = andnot_or(f[4], p1.x, x0);
-                x1 = andnot_or(f[4], q1.x, x1);
-                x2 = andnot_or(f[4], r1.x, x2);
-                x3 = andnot_or(f[4], u1.x, x3);
-                x0 = andnot_or(f[5], p1.y, x0);
-                x1 = andnot_or(f[5], q1.y, x1);
-                x2 = andnot_or(f[5], r1.y, x2);
-                x3 = andnot_or(f[5], u1.y, x3);
-                // common case: no hit among the four (one min chain, one vote)
-                if (!__any_sync(kFull, lane_valid && min(min(x0, x1), min(x2, x3)) == 0)) continue;
-                // warp-uniform from here: one ballot per candidate gives the
-                // tile's hit mask for that query; lane k < 4 stages record k
-                // (list padding reads the stage's pad record: query id
-                // kPadQuery, dropped by the key gather)
-                const uint32_t b0 = __ballot_sync(kFull, x0 == 0) & vm;
-                const uint32_t b1 = __ballot_sync(kFull, x1 == 0) & vm;
-                const uint32_t b2 = __ballot_sync(kFull, x2 == 0) & vm;
-                const uint32_t b3 = __ballot_sync(kFull, x3 == 0) & vm;
-                const uint32_t mine = lane == 0 ? b0 : lane == 1 ? b1 : lane == 2 ? b2 : b3;
-                const uint32_t qid = lane == 0 ? p1.z : lane == 1 ? q1.z : lane == 2 ? r1.z : u1.z;
-                const bool w = lane < 4 && mine != 0;
-                const uint32_t wm = __ballot_sync(kFull, w);
-                if (wn + 4 > (uint32_t)kWarpRecs) {
-                    flush_recs(s_rec[warp], wn, a, lane);
-                    wn = 0;
+            const uint32_t vm = ti.count >= 32u ? kFull : (1u << ti.count) - 1u;  // lanes holding a filter
+            const uint32_t groups = (ti.count + 3) >> 2;
+            const bool per_query = ((n + 31) >> 5) * (16u + 40u * groups) < ((n + 3) >> 2) * a.fpl_trip_cost;
+            if (per_query) {
+#pragma unroll
+                for (int k = 0; k < kWords; ++k) tfw[k * kTile + lane] = f[k];
+                __syncwarp();
+                for (uint32_t p0 = 0; p0 < n; p0 += 32) {
+                    if (COUNT) {
+                        ++w_passes;
+                        w_groups += groups;
+                    }
+                    const uint32_t i = p0 + lane;
+                    const uint32_t c2 = i < n ? list[i] : kChunk * 2;
+                    const uint4 qa = sq[c2], qb = sq[c2 + 1];
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int g = 0; g < kTile / 4; ++g) {
+                        if (g >= (int)groups) break;
+                        const uint4 w0 = S.tf[warp][0][g], w1 = S.tf[warp][1][g], w2 = S.tf[warp][2][g];
+                        const uint4 w3 = S.tf[warp][3][g], w4 = S.tf[warp][4][g], w5 = S.tf[warp][5][g];
+                        uint32_t x0 = w0.x & ~qa.x, x1 = w0.y & ~qa.x, x2 = w0.z & ~qa.x, x3 = w0.w & ~qa.x;
+                        x0 = andnot_or(w1.x, qa.y, x0);
+                        x1 = andnot_or(w1.y, qa.y, x1);
+                        x2 = andnot_or(w1.z, qa.y, x2);
+                        x3 = andnot_or(w1.w, qa.y, x3);
+                        x0 = andnot_or(w2.x, qa.z, x0);
+                        x1 = andnot_or(w2.y, qa.z, x1);
+                        x2 = andnot_or(w2.z, qa.z, x2);
+                        x3 = andnot_or(w2.w, qa.z, x3);
+                        x0 = andnot_or(w3.x, qa.w, x0);
+                        x1 = andnot_or(w3.y, qa.w, x1);
+                        x2 = andnot_or(w3.z, qa.w, x2);
+                        x3 = andnot_or(w3.w, qa.w, x3);
+                        x0 = andnot_or(w4.x, qb.x, x0);
+                        x1 = andnot_or(w4.y, qb.x, x1);
+                        x2 = andnot_or(w4.z, qb.x, x2);
+                        x3 = andnot_or(w4.w, qb.x, x3);
+                        x0 = andnot_or(w5.x, qb.y, x0);
+                        x1 = andnot_or(w5.y, qb.y, x1);
+                        x2 = andnot_or(w5.z, qb.y, x2);
+                        x3 = andnot_or(w5.w, qb.y, x3);
+                        if (x0 == 0) m |= 1u << (4 * g);
+                        if (x1 == 0) m |= 2u << (4 * g);
+                        if (x2 == 0) m |= 4u << (4 * g);
+                        if (x3 == 0) m |= 8u << (4 * g);
+                    }
+                    m &= vm;
+                    if (i >= n) m = 0;
+                    const uint32_t wm = __ballot_sync(kFull, m != 0);
+                    if (wm == 0) continue;
+                    if (wn + 32 > (uint32_t)kWarpRecs) {
+                        flush_recs(S.rec[warp], wn, a, lane);
+                        wn = 0;
+                    }
+                    if (m) {
+                        const uint32_t nk = mask_keys(a.tile_keys[t], m, a.slot_key_off, t);
+                        S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qb.z, t, m, nk};
+                        atomicAdd(&a.qkeys[qb.z], nk);
+                        pairs += __popc(m);
+                    }
+                    wn += __popc(wm);
                 }
-                if (w) s_rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qid, t, mine, 0u};
-                wn += __popc(wm);
+            } else {
+                const bool lane_valid = lane < ti.count;
+                __syncwarp();
+                for (uint32_t i = 0; i < n; i += 4) {
+                    if (COUNT) ++w_trips;
+                    const uint4 idx = *reinterpret_cast<const uint4 *>(&list[i]);
+                    const uint4 p0 = sq[idx.x], p1 = sq[idx.x + 1];
+                    const uint4 q0 = sq[idx.y], q1 = sq[idx.y + 1];
+                    const uint4 r0 = sq[idx.z], r1 = sq[idx.z + 1];
+                    const uint4 u0 = sq[idx.w], u1 = sq[idx.w + 1];
+                    uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
+                    x0 = andnot_or(f[1], p0.y, x0);
+                    x1 = andnot_or(f[1], q0.y, x1);
+                    x2 = andnot_or(f[1], r0.y, x2);
+                    x3 = andnot_or(f[1], u0.y, x3);
+                    x0 = andnot_or(f[2], p0.z, x0);
+                    x1 = andnot_or(f[2], q0.z, x1);
+                    x2 = andnot_or(f[2], r0.z, x2);
+                    x3 = andnot_or(f[2], u0.z, x3);
+                    x0 = andnot_or(f[3], p0.w, x0);
+                    x1 = andnot_or(f[3], q0.w, x1);
+                    x2 = andnot_or(f[3], r0.w, x2);
+                    x3 = andnot_or(f[3], u0.w, x3);
+                    x0 = andnot_or(f[4], p1.x, x0);
+                    x1 = andnot_or(f[4], q1.x, x1);
+                    x2 = andnot_or(f[4], r1.x, x2);
+                    x3 = andnot_or(f[4], u1.x, x3);
+                    x0 = andnot_or(f[5], p1.y, x0);
+                    x1 = andnot_or(f[5], q1.y, x1);
+                    x2 = andnot_or(f[5], r1.y, x2);
+                    x3 = andnot_or(f[5], u1.y, x3);
+                    // common case: no hit among the four (one min chain, one vote)
+                    if (!__any_sync(kFull, lane_valid && min(min(x0, x1), min(x2, x3)) == 0)) continue;
+                    // warp-uniform from here: one ballot per candidate gives the
+                    // tile's hit mask for that query; lane k < 4 stages record k
+                    // (list padding points at the pad record and is dropped)
+                    const uint32_t b0 = __ballot_sync(kFull, x0 == 0) & vm;
+                    const uint32_t b1 = __ballot_sync(kFull, x1 == 0) & vm;
+                    const uint32_t b2 = __ballot_sync(kFull, x2 == 0) & vm;
+                    const uint32_t b3 = __ballot_sync(kFull, x3 == 0) & vm;
+                    const uint32_t mine = lane == 0 ? b0 : lane == 1 ? b1 : lane == 2 ? b2 : b3;
+                    const uint32_t qid = lane == 0 ? p1.z : lane == 1 ? q1.z : lane == 2 ? r1.z : u1.z;
+                    const bool w = lane < 4 && mine != 0 && i + lane < n;
+                    const uint32_t wm = __ballot_sync(kFull, w);
+                    if (wm == 0) continue;
+                    if (wn + 4 > (uint32_t)kWarpRecs) {
+                        flush_recs(S.rec[warp], wn, a, lane);
+                        wn = 0;
+                    }
+                    if (w) {
+                        const uint32_t nk = mask_keys(a.tile_keys[t], mine, a.slot_key_off, t);
+                        S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qid, t, mine, nk};
+                        atomicAdd(&a.qkeys[qid], nk);
+                        pairs += __popc(mine);
+                    }
+                    wn += __popc(wm);
+                }
             }
-            __syncwarp();  // the list is rebuilt for the next tile
+            __syncwarp();  // the list and the tile buffer are rebuilt for the next tile
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[b]);
+        if (lane == 0) mbar_arrive(&S.empty[b]);
     }
-    if (wn) flush_recs(s_rec[warp], wn, a, lane);
+    if (wn) flush_recs(S.rec[warp], wn, a, lane);
+    pairs = __reduce_add_sync(kFull, pairs);
+    if (lane == 0 && pairs) atomicAdd(&a.counters[3], (unsigned long long)pairs);
     if (COUNT && lane == 0) {
         atomicAdd(&a.work[0], (unsigned long long)w_tiles);
-        atomicAdd(&a.work[1], (unsigned long long)w_bits);
+        atomicAdd(&a.work[1], (unsigned long long)w_passes);
         atomicAdd(&a.work[2], (unsigned long long)w_cand);
         atomicAdd(&a.work[3], (unsigned long long)w_trips);
+        atomicAdd(&a.work[5], (unsigned long long)w_groups);
         if (warp == 0) atomicAdd(&a.work[4], (unsigned long long)w_items);
     }
+    // no copy may still target this CTA's shared memory when it exits: after
+    // a failed wait, wait (bounded) for the copies still in flight
+    if (tid == 0) {
+        for (int s = 0; s < 2; ++s)
+            if (((S.inflight >> s) & 1) && !mbar_wait(&S.full[s], (S.inflight_par >> s) & 1))
+                atomicOr(&a.counters[2], 4ull);
+    }
+}
+
+// Launches the subset test on grid CTAs (its shared memory is above the
+// 48 KB static limit, so the size is set on the kernel first).
+template <bool COUNT>
+inline void launch_match(const MatchArgs &a, unsigned grid, cudaStream_t st) {
+    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(MatchSmem))));
+    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared)));
+    k_match<COUNT><<<grid, kMatchThreads, sizeof(MatchSmem), st>>>(a);
 }
 
 // ---------------------------------------------------------------------------
 // Key gather
 // ---------------------------------------------------------------------------
-// Keys of the filters in a hit mask.  The table keeps keys in slot order, so
-// a run of adjacent set bits [lo, hi) is the one key range [o[lo], o[hi])
-// (o: the tile's slot key offsets, 33 of them).  Calls f(begin, end) per run.
-template <class F>
-__device__ __forceinline__ void for_each_key_run(const uint32_t *__restrict__ o, uint32_t mask, F f) {
-    uint64_t m = mask;
-    while (m) {
-        const int lo = __ffsll(m) - 1;
-        const uint64_t filled = m + (1ull << lo);  // the carry clears the run and sets bit hi
-        const int hi = __ffsll(filled & ~m) - 1;
-        f(o[lo], o[hi]);
-        m &= filled;
-    }
-}
+constexpr int kFillPerLane = 4;  // records per lane per warp step (loads in flight)
 
-// Per-query key totals (qkeys, zeroed by the caller), one atomic per
-// record; each record keeps its own total in nkeys for the fill.  Also
-// counts the matching (query, filter) pairs (counters[3]).  Records of the
-// pad query (candidate-list padding) are skipped.
-__global__ void k_key_count(HitRec *__restrict__ recs, unsigned long long *__restrict__ counters,
-                            const uint32_t *__restrict__ slot_key_off, uint32_t *__restrict__ qkeys) {
-    const unsigned long long n = counters[1];
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    uint32_t pairs = 0;
-    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const HitRec r = recs[i];
-        if (r.query == kPadQuery) continue;
-        uint32_t nk = 0;
-        for_each_key_run(slot_key_off + size_t(r.tile) * kTile, r.mask, [&](uint32_t b, uint32_t e) { nk += e - b; });
-        recs[i].nkeys = nk;
-        atomicAdd(&qkeys[r.query], nk);
-        pairs += __popc(r.mask);
-    }
-    pairs = __reduce_add_sync(kFull, pairs);
-    if ((threadIdx.x & 31) == 0 && pairs) atomicAdd(&counters[3], (unsigned long long)pairs);
-}
-
-// Copies every record's keys into its query's range (qoff).  Each lane
-// reserves its record's keys with one atomic on the query's cursor
-// (qcursor, zeroed by the caller).  Records whose hits form one run of
+// Copies every record's keys into its query's range (qoff).  Each record's
+// keys are reserved with one atomic on the query's cursor (qcursor, zeroed
+// by the caller).  A warp takes 4 x 32 records per step, so that the four
+// dependent load levels (record -> cursor and key start -> keys) each have
+// four requests in flight per lane.  Records whose hits form one run of
 // adjacent bits (the usual case) have one contiguous key range; the warp
-// copies those ranges together, 32 keys per step: a prefix sum over the
-// lanes' key counts, and for key j of the warp a 5-step shuffle search for
-// the lane that owns it.  Records with several runs copy their own ranges.
-__global__ void k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
-                           const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
-                           const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor, uint32_t *__restrict__ out) {
+// copies the ranges of 32 such records together, 32 keys per step: a prefix
+// sum over the lanes' key counts, and for key j of the warp a 5-step shuffle
+// search for the lane that owns it.  Records with several runs copy their
+// own ranges.
+__global__ void __launch_bounds__(256) k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
+                                                  const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
+                                                  const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor,
+                                                  uint32_t *__restrict__ out) {
     const unsigned long long n = counters[1];
     const unsigned lane = threadIdx.x & 31;
     const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
-    for (unsigned long long base = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x - lane); base < n;
-         base += warps * 32) {
-        const unsigned long long i = base + lane;
-        HitRec r{kPadQuery, 0u, 0u, 0u};
-        if (i < n) r = recs[i];
-        const uint32_t nk = r.query == kPadQuery ? 0u : r.nkeys;
-        const uint32_t *o = slot_key_off + size_t(r.tile) * kTile;
-        const uint32_t lo = nk ? uint32_t(__ffs(r.mask)) - 1 : 0u;
-        const uint32_t run = r.mask >> lo;
-        const bool single = nk && (run & (run + 1)) == 0;  // one run of adjacent bits
-        uint32_t src = single ? __ldg(&o[lo]) : 0u;
-        uint64_t dst = 0;
-        if (nk) dst = qoff[r.query] + atomicAdd(&qcursor[r.query], nk);
-        // several runs: this lane copies its own ranges
-        if (nk && !single) {
-            uint32_t *d = out + dst;
-            for_each_key_run(o, r.mask, [&](uint32_t b, uint32_t e) {
-                for (uint32_t k = b; k < e; ++k) *d++ = tkeys[k];
-            });
-        }
-        // one run: the warp copies all such ranges together
-        const uint32_t cnk = single ? nk : 0u;
-        uint32_t incl = cnk;
+    const unsigned long long wid = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    constexpr unsigned kStep = 32 * kFillPerLane;
+    for (unsigned long long base = wid * kStep; base < n; base += warps * kStep) {
+        HitRec r[kFillPerLane];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t v = __shfl_up_sync(kFull, incl, d);
-            if (lane >= (unsigned)d) incl += v;
+        for (int j = 0; j < kFillPerLane; ++j) {
+            const unsigned long long i = base + j * 32 + lane;
+            r[j] = i < n ? recs[i] : HitRec{kPadQuery, 0u, 0u, 0u};
         }
-        const uint32_t total = __shfl_sync(kFull, incl, 31);
-        const uint32_t start = incl - cnk;  // this lane's first key among the warp's
-        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
-            const uint32_t j = j0 + lane;
-            // owner: the first lane whose inclusive count exceeds j
-            uint32_t owner = 0;
+        uint32_t nk[kFillPerLane], src[kFillPerLane];
+        uint64_t dst[kFillPerLane];
+        bool single[kFillPerLane];
 #pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
-                if (v <= j) owner += step;
+        for (int j = 0; j < kFillPerLane; ++j) {
+            nk[j] = r[j].query == kPadQuery ? 0u : r[j].nkeys;
+            dst[j] = 0;
+            if (nk[j]) dst[j] = qoff[r[j].query] + atomicAdd(&qcursor[r[j].query], nk[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < kFillPerLane; ++j) {
+            const uint32_t lo = nk[j] ? uint32_t(__ffs(r[j].mask)) - 1 : 0u;
+            const uint32_t run = r[j].mask >> lo;
+            single[j] = nk[j] && (run & (run + 1)) == 0;  // one run of adjacent bits
+            src[j] = single[j] ? __ldg(&slot_key_off[size_t(r[j].tile) * kTile + lo]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kFillPerLane; ++j) {
+            // several runs: this lane copies its own ranges
+            if (nk[j] && !single[j]) {
+                const uint32_t *o = slot_key_off + size_t(r[j].tile) * kTile;
+                uint64_t d = dst[j];
+                uint64_t m = r[j].mask;
+                while (m) {  // runs of adjacent hit bits, as in for_each_key_run
+                    const int lo = __ffsll(m) - 1;
+                    const uint64_t filled = m + (1ull << lo);
+                    const int hi = __ffsll(filled & ~m) - 1;
+                    for (uint32_t k = o[lo], e = o[hi]; k < e; ++k) out[d++] = tkeys[k];
+                    m &= filled;
+                }
             }
-            const uint32_t ostart = __shfl_sync(kFull, start, owner);
-            const uint32_t osrc = __shfl_sync(kFull, src, owner);
-            const uint64_t odst = __shfl_sync(kFull, dst, owner);
-            if (j < total) out[odst + (j - ostart)] = tkeys[osrc + (j - ostart)];
+            // one run: the warp copies all such ranges together
+            const uint32_t cnk = single[j] ? nk[j] : 0u;
+            uint32_t incl = cnk;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t v = __shfl_up_sync(kFull, incl, d);
+                if (lane >= (unsigned)d) incl += v;
+            }
+            const uint32_t total = __shfl_sync(kFull, incl, 31);
+            const uint32_t start = incl - cnk;  // this lane's first key among the warp's
+            for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+                const uint32_t k = j0 + lane;
+                // owner: the first lane whose inclusive count exceeds k
+                uint32_t owner = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
+                    if (v <= k) owner += step;
+                }
+                const uint32_t ostart = __shfl_sync(kFull, start, owner);
+                const uint32_t osrc = __shfl_sync(kFull, src[j], owner);
+                const uint64_t odst = __shfl_sync(kFull, dst[j], owner);
+                if (k < total) out[odst + (k - ostart)] = tkeys[osrc + (k - ostart)];
+            }
         }
     }
 }

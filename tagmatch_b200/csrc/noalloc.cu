@@ -72,6 +72,8 @@ struct Arena {
         used = off + bytes;
         return reinterpret_cast<T *>(base + off);
     }
+    // gives back everything taken after end (end: one past the last byte kept)
+    void trim(const void *end) { used = size_t(static_cast<const unsigned char *>(end) - base); }
     size_t left() const {
         const size_t off = (used + 255) & ~size_t(255);
         return off < kNoAllocScratchBytes ? kNoAllocScratchBytes - off : 0;
@@ -185,14 +187,15 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         k_slices<<<chunks, kChunk, 0, st>>>(queue, part_off, part_count, chunk_off, P, slices);
         TM_CHECK_LAUNCH();
     }
-    // hit records fill what is left of the array (a quarter of it is kept
-    // back for the match_unique key buffer)
-    const size_t rec_room = (unique ? ar.left() * 3 / 4 : ar.left()) / sizeof(HitRec);
+    // hit records fill what is left of the array; after the match the part
+    // they did not use goes to the keys
+    const size_t rec_room = ar.left() / sizeof(HitRec);
     if (rec_room < 256) throw Error(TM_ERR_CAPACITY, "no-allocation scratch exhausted before the hit records; split the batch");
     HitRec *recs = ar.take<HitRec>(rec_room - 32, "hit records");
-    MatchArgs a{t.tile_words.p, t.tile_info.p, t.part_tile_begin.p, part_count, part_off, item_off, chunk_off, queue, slices,
-                P, seg_tiles, counters, recs, (unsigned long long)(rec_room - 32), nullptr};
-    k_match<false><<<unsigned(sms) * 4, kMatchThreads, 0, st>>>(a);
+    MatchArgs a{t.tile_words.p, t.tile_info.p, t.tile_keys.p, t.slot_key_off.p, t.part_tile_begin.p, part_count, part_off,
+                item_off, chunk_off, queue, slices, P, seg_tiles, counters, recs, (unsigned long long)(rec_room - 32), qkeys,
+                fpl_trip_cost(), nullptr};
+    launch_match<false>(a, unsigned(sms) * 4, st);
     TM_CHECK_LAUNCH();
     unsigned long long hc[3] = {0, 0, 0};
     TM_CUDA(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, st));
@@ -203,9 +206,8 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
                                          " hit records of this batch; split the batch");
 
     // keys
-    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256), unsigned(sms) * 16));
-    k_key_count<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, qkeys);
-    TM_CHECK_LAUNCH();
+    ar.trim(recs + hc[1]);
+    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256 * kFillPerLane), unsigned(sms) * 16));
     uint64_t *key_off = unique ? qoff : d_out_offsets;
     scan_fixed<uint32_t, uint64_t>(qkeys, key_off, nq, sums, offs, st);
     uint64_t total = 0;
@@ -221,11 +223,15 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         return;
     }
     // match_unique: keys into one arena buffer, de-duplicated into a second
-    // one, then compacted into the caller's output
+    // one (the hit records' space when it is large enough: they are no
+    // longer read once the keys are filled), then compacted into the
+    // caller's output
     const uint64_t bitmap_words = (uint64_t(t.max_key) >> 5) + 1;
     const bool bitmap = bitmap_words * 4 <= 48 * 1024;
     uint32_t *keys = ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
-    uint32_t *ukeys = ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
+    uint32_t *ukeys = std::max<uint64_t>(total, 1) * sizeof(uint32_t) <= hc[1] * sizeof(HitRec)
+                          ? reinterpret_cast<uint32_t *>(recs)
+                          : ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
     k_key_fill<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, t.keys.p, qoff, qcursor, keys);
     TM_CHECK_LAUNCH();
     if (bitmap) {

@@ -589,6 +589,21 @@ __global__ void k_slot_keys(const uint32_t *__restrict__ slot_filter, size_t n_s
     for (uint32_t k = b; k < e; ++k) out_keys[d++] = keys[k];
 }
 
+// One warp per tile: the key counts of its lanes' filters as bit planes.
+__global__ void k_tile_keys(const uint32_t *__restrict__ slot_key_off, uint32_t n_tiles, TileKeys *__restrict__ out) {
+    const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = threadIdx.x & 31;
+    if (t >= n_tiles) return;
+    const size_t s = size_t(t) * kTile + lane;
+    const uint32_t nk = slot_key_off[s + 1] - slot_key_off[s];
+    TileKeys tk;
+    tk.p[0] = __ballot_sync(kFull, nk < 8 && (nk & 1));
+    tk.p[1] = __ballot_sync(kFull, nk < 8 && (nk & 2));
+    tk.p[2] = __ballot_sync(kFull, nk < 8 && (nk & 4));
+    tk.wide = __ballot_sync(kFull, nk >= 8);
+    if (lane == 0) out[t] = tk;
+}
+
 __global__ void k_max_key(const uint32_t *__restrict__ keys, size_t n, uint32_t *__restrict__ out) {
     uint32_t m = 0;
     for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
@@ -601,7 +616,8 @@ __global__ void k_max_key(const uint32_t *__restrict__ keys, size_t n, uint32_t 
 
 size_t DevTable::device_bytes() const {
     return tile_words.cap * sizeof(uint32_t) + tile_info.cap * sizeof(TileInfo) + tile_and.cap * 4 + part_tile_begin.cap * 4 +
-           part_mask.cap * 4 + slot_key_off.cap * 4 + keys.cap * 4 + slot_filter.cap * 4;
+           part_mask.cap * 4 + slot_key_off.cap * 4 + tile_keys.cap * sizeof(TileKeys) + keys.cap * 4 +
+           slot_filter.cap * 4;
 }
 
 void build_table(const PartitionResult &pr, const uint32_t *d_key_off, const uint32_t *d_keys, uint64_t n_keys, DevTable &t,
@@ -674,6 +690,11 @@ void build_table(const PartitionResult &pr, const uint32_t *d_key_off, const uin
     if (n_slots) {
         k_slot_keys<<<blocks_for(n_slots, 256), 256, 0, st>>>(t.slot_filter.p, n_slots, d_key_off, d_keys, t.slot_key_off.p,
                                                              t.keys.p);
+        TM_CHECK_LAUNCH();
+    }
+    t.tile_keys.reserve(std::max<uint32_t>(nt, 1));
+    if (nt) {
+        k_tile_keys<<<blocks_for(size_t(nt) * 32, 256), 256, 0, st>>>(t.slot_key_off.p, nt, t.tile_keys.p);
         TM_CHECK_LAUNCH();
     }
     DevBuf<uint32_t> mk;

@@ -46,6 +46,7 @@ struct DevTable {
     DevBuf<uint32_t> part_tile_begin; // [n_parts + 1]
     DevBuf<uint32_t> part_mask;       // [n_parts][8]: 6 mask words, tile count, pad
     DevBuf<uint32_t> slot_key_off;    // [n_tiles * 32 + 1]
+    DevBuf<TileKeys> tile_keys;       // [n_tiles] key counts per lane as bit planes
     DevBuf<uint32_t> keys;            // [n_keys]
     DevBuf<uint32_t> slot_filter;     // [n_tiles * 32] original filter index (0xFFFFFFFF for empty lanes)
     std::vector<uint32_t> h_part_mask;  // host copy of the masks [n_parts][8]

@@ -30,14 +30,28 @@ struct __align__(16) TileInfo {
 };
 
 // One candidate query's hits in one tile: bit l of mask is set when the
-// tile's filter in lane l (slot tile * 32 + l) matches the query.  nkeys is
-// filled in by the key count (the keys of those filters).
+// tile's filter in lane l (slot tile * 32 + l) matches the query; nkeys is
+// the number of keys of those filters.
 struct __align__(16) HitRec {
     uint32_t query;
     uint32_t tile;
     uint32_t mask;
     uint32_t nkeys;
 };
+
+// Key counts of a tile's filters as bit planes, so that the keys of any
+// hit mask m are popc(m & p[0]) + 2 popc(m & p[1]) + 4 popc(m & p[2]):
+// bit l of p[b] is bit b of the key count of the filter in lane l, for
+// counts below 8.  Bit l of wide is set when that filter has 8 keys or
+// more; masks that touch such lanes are counted from the slot offsets.
+struct __align__(16) TileKeys {
+    uint32_t p[3];
+    uint32_t wide;
+};
+
+__device__ __forceinline__ uint32_t keys_of_mask(const TileKeys &tk, uint32_t m) {
+    return __popc(m & tk.p[0]) + 2u * __popc(m & tk.p[1]) + 4u * __popc(m & tk.p[2]);
+}
 
 __device__ __forceinline__ uint32_t andnot_or(uint32_t f, uint32_t q, uint32_t acc) {
     return (f & ~q) | acc;  // one LOP3
