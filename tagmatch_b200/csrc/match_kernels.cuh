@@ -13,6 +13,7 @@ constexpr int kRouteThreads = 256;
 constexpr int kMatchThreads = 256;
 constexpr int kMatchWarps = kMatchThreads / 32;
 constexpr int kWarpRecs = 64;  // staged hit records per warp (1 KB)
+constexpr int kQuad = 4;       // tiles a warp selects candidates for at once
 constexpr uint32_t kMaxRouteParts = 1536;  // partition masks per routing window (48 KB of shared memory)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
@@ -223,7 +224,8 @@ struct __align__(128) Stage {
 struct MatchSmem {
     Stage st[2];
     HitRec rec[kMatchWarps][kWarpRecs];                  // staged hit records per warp
-    uint32_t list[kMatchWarps][kChunk + 8];              // candidate lists per warp
+    uint8_t list[kMatchWarps][kQuad][kChunk + 8];        // candidate lists (query index in the chunk) per warp and tile
+    TileKeys tk[kMatchWarps][kQuad];                     // key-count planes of the warp's four tiles
     uint4 tf[kMatchWarps][kWords][kTile / 4];            // a warp's tile: word k of filters 4 g .. 4 g + 3
     uint64_t full[2], empty[2];
     uint32_t item[2];
@@ -294,12 +296,14 @@ __device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, Matc
 // The subset test.  Persistent CTAs take work items (partition, 256-query
 // chunk, segment of the partition's tiles) from an atomic counter; thread 0
 // stages each item's query records and slices with bulk TMA copies into one
-// of two buffers while the CTA matches the other.  Each warp takes one tile
-// (<= 32 filters) at a time:
-//  * selection: the tile's 8 selector bits (bits every member holds); lanes
-//    0-7 OR the "lacks bit" slices of their 32-query word, so a query that
-//    lacks any of them is dropped; the remaining candidates are written to
-//    the warp's list (lane l compacts byte l & 3 of word l >> 2);
+// of two buffers while the CTA matches the other.  Each warp takes four
+// tiles (<= 32 filters each) at a time:
+//  * selection, for the four tiles at once: the tile's 8 selector bits
+//    (bits every member holds); lane l ORs the "lacks bit" slices of 32-query
+//    word l & 7 for tile l >> 3, so a query that lacks any of them is
+//    dropped; the remaining candidates go to the tile's list (one byte per
+//    query, placed by a prefix sum over the tile's 8 words);
+// then, tile by tile:
 //  * many candidates: one candidate query per lane, the tile's filters read
 //    from shared memory (one broadcast 128-bit load gives word k of four
 //    filters): 6 LOP3 per (query, filter), the lane's hit mask over the tile
@@ -341,7 +345,6 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     uint32_t wn = 0;     // records staged by this warp (warp-uniform)
     uint32_t pairs = 0;  // matching (query, filter) pairs found by this lane
     const uint32_t lane_lt = (1u << lane) - 1u;
-    uint32_t *list = S.list[warp];
     uint32_t *tfw = reinterpret_cast<uint32_t *>(S.tf[warp]);
     for (uint32_t it = 0;; ++it) {
         const int b = it & 1;
@@ -372,169 +375,181 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
         if (COUNT) ++w_items;
         const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[b].q);
         const uint32_t *sz = S.st[b].z;
-        for (uint32_t t = r.tb + warp; t < r.te; t += kMatchWarps) {
-            const TileInfo ti = a.tile_info[t];
-            uint32_t f[kWords];
-#pragma unroll
-            for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
-            if (COUNT) ++w_tiles;
-            // candidates: queries holding the tile's selection bits; lane
-            // w < 8 ORs the "lacks" slices for queries 32 w .. 32 w + 31
-            uint32_t cand_word = 0;
-            if (lane < 8) {
-                const uint32_t *zl = sz + lane;
+        for (uint32_t t0 = r.tb + warp * kQuad; t0 < r.te; t0 += kMatchWarps * kQuad) {
+            // selection for four tiles at once: lane l serves word l & 7 of
+            // tile t0 + (l >> 3); the tile's 8 selector bits OR the "lacks"
+            // slices of the lane's 32 queries
+            const uint32_t gi = lane >> 3, w = lane & 7;
+            const uint32_t tq = t0 + gi;
+            uint32_t cand = 0, tcount = 0;
+            if (tq < r.te) {
+                const TileInfo ti = a.tile_info[tq];
+                tcount = ti.count;
+                const uint32_t *zl = sz + w;
                 const uint32_t lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
                                       zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] |
                                       zl[(ti.sel[1] & 0xFFu) * 8] | zl[((ti.sel[1] >> 8) & 0xFFu) * 8] |
                                       zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
-                cand_word = ~lack;
-                if (lane * 32 + 32 > r.nq) cand_word &= lane * 32 >= r.nq ? 0u : ((1u << (r.nq - lane * 32)) - 1u);
+                cand = ~lack;
+                if (w * 32 + 32 > r.nq) cand &= w * 32 >= r.nq ? 0u : ((1u << (r.nq - w * 32)) - 1u);
+                if (w == 0) S.tk[warp][gi] = a.tile_keys[tq];
             }
-            // compact candidate list (uint4 index of each query record):
-            // lane l writes the candidates of byte l & 3 of word l >> 2
-            const uint32_t cw = __shfl_sync(kFull, cand_word, lane >> 2);
-            uint32_t byte = (cw >> ((lane & 3) * 8)) & 0xFFu;
-            const uint32_t cnt = __popc(byte);
+            if (COUNT) w_tiles += __popc(__ballot_sync(kFull, tq < r.te && w == 0));  // lane 0 reports
+            // candidate lists (query index in the chunk, one byte each): a
+            // prefix sum over each tile's 8 words places every lane's queries
+            const uint32_t cnt = __popc(cand);
             uint32_t incl = cnt;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
+            for (int o = 1; o < 8; o <<= 1) {
                 const uint32_t v = __shfl_up_sync(kFull, incl, o);
-                if (lane >= (unsigned)o) incl += v;
+                if (w >= (unsigned)o) incl += v;
             }
-            const uint32_t n = __shfl_sync(kFull, incl, 31);
-            if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
-            if (n == 0) continue;
             {
+                uint8_t *lst = S.list[warp][gi];
                 uint32_t pos = incl - cnt;
-                const uint32_t q0 = (lane >> 2) * 32 + (lane & 3) * 8;
-                while (byte) {
-                    list[pos++] = (q0 + __ffs(byte) - 1) * 2;
-                    byte &= byte - 1;
+                while (cand) {
+                    lst[pos++] = uint8_t(w * 32 + __ffs(cand) - 1);
+                    cand &= cand - 1;
                 }
-                if (lane < 4) list[n + lane] = kChunk * 2;  // pad to a multiple of 4: the stage's pad record
+                const uint32_t nt = __shfl_sync(kFull, incl, lane | 7);
+                if (w < 4) lst[nt + w] = 0;  // pad to a multiple of 4 (query 0; its hits are dropped)
             }
-            const uint32_t vm = ti.count >= 32u ? kFull : (1u << ti.count) - 1u;  // lanes holding a filter
-            const uint32_t groups = (ti.count + 3) >> 2;
-            const bool per_query = ((n + 31) >> 5) * (16u + 40u * groups) < ((n + 3) >> 2) * a.fpl_trip_cost;
-            if (per_query) {
+            __syncwarp();
+            for (int i = 0; i < kQuad; ++i) {
+                const uint32_t n = __shfl_sync(kFull, incl, 8 * i + 7);
+                if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
+                if (n == 0) continue;
+                const uint32_t t = t0 + i;
+                const uint32_t count = __shfl_sync(kFull, tcount, 8 * i);
+                const uint8_t *lst = S.list[warp][i];
+                uint32_t f[kWords];
 #pragma unroll
-                for (int k = 0; k < kWords; ++k) tfw[k * kTile + lane] = f[k];
-                __syncwarp();
-                for (uint32_t p0 = 0; p0 < n; p0 += 32) {
-                    if (COUNT) {
-                        ++w_passes;
-                        w_groups += groups;
-                    }
-                    const uint32_t i = p0 + lane;
-                    const uint32_t c2 = i < n ? list[i] : kChunk * 2;
-                    const uint4 qa = sq[c2], qb = sq[c2 + 1];
-                    uint32_t m = 0;
+                for (int k = 0; k < kWords; ++k) f[k] = __ldg(&a.tile_words[(size_t(t) * kWords + k) * kTile + lane]);
+                const uint32_t vm = count >= 32u ? kFull : (1u << count) - 1u;  // lanes holding a filter
+                const uint32_t groups = (count + 3) >> 2;
+                const bool per_query = ((n + 31) >> 5) * (16u + 40u * groups) < ((n + 3) >> 2) * a.fpl_trip_cost;
+                if (per_query) {
 #pragma unroll
-                    for (int g = 0; g < kTile / 4; ++g) {
-                        if (g >= (int)groups) break;
-                        const uint4 w0 = S.tf[warp][0][g], w1 = S.tf[warp][1][g], w2 = S.tf[warp][2][g];
-                        const uint4 w3 = S.tf[warp][3][g], w4 = S.tf[warp][4][g], w5 = S.tf[warp][5][g];
-                        uint32_t x0 = w0.x & ~qa.x, x1 = w0.y & ~qa.x, x2 = w0.z & ~qa.x, x3 = w0.w & ~qa.x;
-                        x0 = andnot_or(w1.x, qa.y, x0);
-                        x1 = andnot_or(w1.y, qa.y, x1);
-                        x2 = andnot_or(w1.z, qa.y, x2);
-                        x3 = andnot_or(w1.w, qa.y, x3);
-                        x0 = andnot_or(w2.x, qa.z, x0);
-                        x1 = andnot_or(w2.y, qa.z, x1);
-                        x2 = andnot_or(w2.z, qa.z, x2);
-                        x3 = andnot_or(w2.w, qa.z, x3);
-                        x0 = andnot_or(w3.x, qa.w, x0);
-                        x1 = andnot_or(w3.y, qa.w, x1);
-                        x2 = andnot_or(w3.z, qa.w, x2);
-                        x3 = andnot_or(w3.w, qa.w, x3);
-                        x0 = andnot_or(w4.x, qb.x, x0);
-                        x1 = andnot_or(w4.y, qb.x, x1);
-                        x2 = andnot_or(w4.z, qb.x, x2);
-                        x3 = andnot_or(w4.w, qb.x, x3);
-                        x0 = andnot_or(w5.x, qb.y, x0);
-                        x1 = andnot_or(w5.y, qb.y, x1);
-                        x2 = andnot_or(w5.z, qb.y, x2);
-                        x3 = andnot_or(w5.w, qb.y, x3);
-                        if (x0 == 0) m |= 1u << (4 * g);
-                        if (x1 == 0) m |= 2u << (4 * g);
-                        if (x2 == 0) m |= 4u << (4 * g);
-                        if (x3 == 0) m |= 8u << (4 * g);
+                    for (int k = 0; k < kWords; ++k) tfw[k * kTile + lane] = f[k];
+                    __syncwarp();
+                    for (uint32_t p0 = 0; p0 < n; p0 += 32) {
+                        if (COUNT) {
+                            ++w_passes;
+                            w_groups += groups;
+                        }
+                        const uint32_t j = p0 + lane;
+                        const uint32_t c2 = j < n ? 2u * lst[j] : 0u;
+                        const uint4 qa = sq[c2], qb = sq[c2 + 1];
+                        uint32_t m = 0;
+#pragma unroll
+                        for (int g = 0; g < kTile / 4; ++g) {
+                            if (g >= (int)groups) break;
+                            const uint4 w0 = S.tf[warp][0][g], w1 = S.tf[warp][1][g], w2 = S.tf[warp][2][g];
+                            const uint4 w3 = S.tf[warp][3][g], w4 = S.tf[warp][4][g], w5 = S.tf[warp][5][g];
+                            uint32_t x0 = w0.x & ~qa.x, x1 = w0.y & ~qa.x, x2 = w0.z & ~qa.x, x3 = w0.w & ~qa.x;
+                            x0 = andnot_or(w1.x, qa.y, x0);
+                            x1 = andnot_or(w1.y, qa.y, x1);
+                            x2 = andnot_or(w1.z, qa.y, x2);
+                            x3 = andnot_or(w1.w, qa.y, x3);
+                            x0 = andnot_or(w2.x, qa.z, x0);
+                            x1 = andnot_or(w2.y, qa.z, x1);
+                            x2 = andnot_or(w2.z, qa.z, x2);
+                            x3 = andnot_or(w2.w, qa.z, x3);
+                            x0 = andnot_or(w3.x, qa.w, x0);
+                            x1 = andnot_or(w3.y, qa.w, x1);
+                            x2 = andnot_or(w3.z, qa.w, x2);
+                            x3 = andnot_or(w3.w, qa.w, x3);
+                            x0 = andnot_or(w4.x, qb.x, x0);
+                            x1 = andnot_or(w4.y, qb.x, x1);
+                            x2 = andnot_or(w4.z, qb.x, x2);
+                            x3 = andnot_or(w4.w, qb.x, x3);
+                            x0 = andnot_or(w5.x, qb.y, x0);
+                            x1 = andnot_or(w5.y, qb.y, x1);
+                            x2 = andnot_or(w5.z, qb.y, x2);
+                            x3 = andnot_or(w5.w, qb.y, x3);
+                            if (x0 == 0) m |= 1u << (4 * g);
+                            if (x1 == 0) m |= 2u << (4 * g);
+                            if (x2 == 0) m |= 4u << (4 * g);
+                            if (x3 == 0) m |= 8u << (4 * g);
+                        }
+                        m &= vm;
+                        if (j >= n) m = 0;
+                        const uint32_t wm = __ballot_sync(kFull, m != 0);
+                        if (wm == 0) continue;
+                        if (wn + 32 > (uint32_t)kWarpRecs) {
+                            flush_recs(S.rec[warp], wn, a, lane);
+                            wn = 0;
+                        }
+                        if (m) {
+                            const uint32_t nk = mask_keys(S.tk[warp][i], m, a.slot_key_off, t);
+                            S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qb.z, t, m, nk};
+                            atomicAdd(&a.qkeys[qb.z], nk);
+                            pairs += __popc(m);
+                        }
+                        wn += __popc(wm);
                     }
-                    m &= vm;
-                    if (i >= n) m = 0;
-                    const uint32_t wm = __ballot_sync(kFull, m != 0);
-                    if (wm == 0) continue;
-                    if (wn + 32 > (uint32_t)kWarpRecs) {
-                        flush_recs(S.rec[warp], wn, a, lane);
-                        wn = 0;
+                } else {
+                    const bool lane_valid = lane < count;
+                    for (uint32_t j = 0; j < n; j += 4) {
+                        if (COUNT) ++w_trips;
+                        const uint32_t idx4 = *reinterpret_cast<const uint32_t *>(lst + j);
+                        const uint32_t ia = (idx4 & 0xFFu) * 2, ib = ((idx4 >> 8) & 0xFFu) * 2;
+                        const uint32_t ic = ((idx4 >> 16) & 0xFFu) * 2, id = (idx4 >> 24) * 2;
+                        const uint4 p0 = sq[ia], p1 = sq[ia + 1];
+                        const uint4 q0 = sq[ib], q1 = sq[ib + 1];
+                        const uint4 r0 = sq[ic], r1 = sq[ic + 1];
+                        const uint4 u0 = sq[id], u1 = sq[id + 1];
+                        uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
+                        x0 = andnot_or(f[1], p0.y, x0);
+                        x1 = andnot_or(f[1], q0.y, x1);
+                        x2 = andnot_or(f[1], r0.y, x2);
+                        x3 = andnot_or(f[1], u0.y, x3);
+                        x0 = andnot_or(f[2], p0.z, x0);
+                        x1 = andnot_or(f[2], q0.z, x1);
+                        x2 = andnot_or(f[2], r0.z, x2);
+                        x3 = andnot_or(f[2], u0.z, x3);
+                        x0 = andnot_or(f[3], p0.w, x0);
+                        x1 = andnot_or(f[3], q0.w, x1);
+                        x2 = andnot_or(f[3], r0.w, x2);
+                        x3 = andnot_or(f[3], u0.w, x3);
+                        x0 = andnot_or(f[4], p1.x, x0);
+                        x1 = andnot_or(f[4], q1.x, x1);
+                        x2 = andnot_or(f[4], r1.x, x2);
+                        x3 = andnot_or(f[4], u1.x, x3);
+                        x0 = andnot_or(f[5], p1.y, x0);
+                        x1 = andnot_or(f[5], q1.y, x1);
+                        x2 = andnot_or(f[5], r1.y, x2);
+                        x3 = andnot_or(f[5], u1.y, x3);
+                        // common case: no hit among the four (one min chain, one vote)
+                        if (!__any_sync(kFull, lane_valid && min(min(x0, x1), min(x2, x3)) == 0)) continue;
+                        // warp-uniform from here: one ballot per candidate gives the
+                        // tile's hit mask for that query; lane k < 4 stages record k
+                        // (list padding repeats query 0 and is dropped)
+                        const uint32_t b0 = __ballot_sync(kFull, x0 == 0) & vm;
+                        const uint32_t b1 = __ballot_sync(kFull, x1 == 0) & vm;
+                        const uint32_t b2 = __ballot_sync(kFull, x2 == 0) & vm;
+                        const uint32_t b3 = __ballot_sync(kFull, x3 == 0) & vm;
+                        const uint32_t mine = lane == 0 ? b0 : lane == 1 ? b1 : lane == 2 ? b2 : b3;
+                        const uint32_t qid = lane == 0 ? p1.z : lane == 1 ? q1.z : lane == 2 ? r1.z : u1.z;
+                        const bool wr = lane < 4 && mine != 0 && j + lane < n;
+                        const uint32_t wm = __ballot_sync(kFull, wr);
+                        if (wm == 0) continue;
+                        if (wn + 4 > (uint32_t)kWarpRecs) {
+                            flush_recs(S.rec[warp], wn, a, lane);
+                            wn = 0;
+                        }
+                        if (wr) {
+                            const uint32_t nk = mask_keys(S.tk[warp][i], mine, a.slot_key_off, t);
+                            S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qid, t, mine, nk};
+                            atomicAdd(&a.qkeys[qid], nk);
+                            pairs += __popc(mine);
+                        }
+                        wn += __popc(wm);
                     }
-                    if (m) {
-                        const uint32_t nk = mask_keys(a.tile_keys[t], m, a.slot_key_off, t);
-                        S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qb.z, t, m, nk};
-                        atomicAdd(&a.qkeys[qb.z], nk);
-                        pairs += __popc(m);
-                    }
-                    wn += __popc(wm);
                 }
-            } else {
-                const bool lane_valid = lane < ti.count;
-                __syncwarp();
-                for (uint32_t i = 0; i < n; i += 4) {
-                    if (COUNT) ++w_trips;
-                    const uint4 idx = *reinterpret_cast<const uint4 *>(&list[i]);
-                    const uint4 p0 = sq[idx.x], p1 = sq[idx.x + 1];
-                    const uint4 q0 = sq[idx.y], q1 = sq[idx.y + 1];
-                    const uint4 r0 = sq[idx.z], r1 = sq[idx.z + 1];
-                    const uint4 u0 = sq[idx.w], u1 = sq[idx.w + 1];
-                    uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
-                    x0 = andnot_or(f[1], p0.y, x0);
-                    x1 = andnot_or(f[1], q0.y, x1);
-                    x2 = andnot_or(f[1], r0.y, x2);
-                    x3 = andnot_or(f[1], u0.y, x3);
-                    x0 = andnot_or(f[2], p0.z, x0);
-                    x1 = andnot_or(f[2], q0.z, x1);
-                    x2 = andnot_or(f[2], r0.z, x2);
-                    x3 = andnot_or(f[2], u0.z, x3);
-                    x0 = andnot_or(f[3], p0.w, x0);
-                    x1 = andnot_or(f[3], q0.w, x1);
-                    x2 = andnot_or(f[3], r0.w, x2);
-                    x3 = andnot_or(f[3], u0.w, x3);
-                    x0 = andnot_or(f[4], p1.x, x0);
-                    x1 = andnot_or(f[4], q1.x, x1);
-                    x2 = andnot_or(f[4], r1.x, x2);
-                    x3 = andnot_or(f[4], u1.x, x3);
-                    x0 = andnot_or(f[5], p1.y, x0);
-                    x1 = andnot_or(f[5], q1.y, x1);
-                    x2 = andnot_or(f[5], r1.y, x2);
-                    x3 = andnot_or(f[5], u1.y, x3);
-                    // common case: no hit among the four (one min chain, one vote)
-                    if (!__any_sync(kFull, lane_valid && min(min(x0, x1), min(x2, x3)) == 0)) continue;
-                    // warp-uniform from here: one ballot per candidate gives the
-                    // tile's hit mask for that query; lane k < 4 stages record k
-                    // (list padding points at the pad record and is dropped)
-                    const uint32_t b0 = __ballot_sync(kFull, x0 == 0) & vm;
-                    const uint32_t b1 = __ballot_sync(kFull, x1 == 0) & vm;
-                    const uint32_t b2 = __ballot_sync(kFull, x2 == 0) & vm;
-                    const uint32_t b3 = __ballot_sync(kFull, x3 == 0) & vm;
-                    const uint32_t mine = lane == 0 ? b0 : lane == 1 ? b1 : lane == 2 ? b2 : b3;
-                    const uint32_t qid = lane == 0 ? p1.z : lane == 1 ? q1.z : lane == 2 ? r1.z : u1.z;
-                    const bool w = lane < 4 && mine != 0 && i + lane < n;
-                    const uint32_t wm = __ballot_sync(kFull, w);
-                    if (wm == 0) continue;
-                    if (wn + 4 > (uint32_t)kWarpRecs) {
-                        flush_recs(S.rec[warp], wn, a, lane);
-                        wn = 0;
-                    }
-                    if (w) {
-                        const uint32_t nk = mask_keys(a.tile_keys[t], mine, a.slot_key_off, t);
-                        S.rec[warp][wn + __popc(wm & lane_lt)] = HitRec{qid, t, mine, nk};
-                        atomicAdd(&a.qkeys[qid], nk);
-                        pairs += __popc(mine);
-                    }
-                    wn += __popc(wm);
-                }
+                __syncwarp();  // the tile buffer is rebuilt for the next tile
             }
-            __syncwarp();  // the list and the tile buffer are rebuilt for the next tile
+            __syncwarp();  // the lists are rebuilt for the next four tiles
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&S.empty[b]);
