@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", type=int, default=1, choices=[1, 2],
+                    help="1: 10M filters (the headline); 2: 100M filters, Zipf s=1.3, superset fractions 10/50/90%%")
     ap.add_argument("--filters", type=int, default=FILTERS)
     ap.add_argument("--queries", type=int, default=QUERIES)
     ap.add_argument("--batch", type=int, default=131072, help="queries per device batch")
@@ -64,7 +66,11 @@ def parse():
     ap.add_argument("--parity-samples", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-rates", default="200000,500000,1000000")
+    ap.add_argument("--serve-rates", default="250000,500000,650000,800000,1000000,2000000")
+    ap.add_argument("--serve-plain-rates", default="100000,150000,200000,300000,450000")
+    ap.add_argument("--serve-modes", default="plain,continuous,learned")
+    ap.add_argument("--latency-target-ms", type=int, default=25)
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned work-queue order comparison")
     ap.add_argument("--serve-seconds", type=float, default=4.0)
     return ap.parse_args()
 
@@ -226,19 +232,192 @@ def parity_check(tm, f, ko, k, q, base, B, unique, stream, samples):
                    + (" + tagmatch_query.hh:99-119 sort/unique" if unique else "")}
 
 
+def learned_order(tm, step, args, stream):
+    """The learned scheduler on the timed workload: two steps recorded as
+    timing samples, the cost model trained on the GPU, then steps with the
+    work queue in the model's order against steps in partition id order
+    (alternating, CUDA events on the matcher's stream)."""
+    import torch
+    tm.sched_record(True)
+    for _ in range(2):
+        step()
+    tm.sched_record(False)
+    rep = tm.sched_train(epochs=30)
+    times = {False: [], True: []}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(2 * max(2, args.steps)):
+        use = bool(i & 1)
+        tm.sched_use_order(use)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times[use].append(e0.elapsed_time(e1))
+    tm.sched_use_order(False)
+    static_ms, learned_ms = statistics.median(times[False]), statistics.median(times[True])
+    return {"model": "8-64-64-1 fp32 MLP, trained by the library's kernels on per-item timing samples",
+            "samples": rep["samples"], "train_steps": rep["steps"], "train_ms": round(rep["ms"], 1),
+            "val_r2": round(rep["val_r2"], 4), "val_mse": round(rep["val_mse"], 4), "mean_mse": round(rep["mean_mse"], 4),
+            "static_order_ms_per_step": round(static_ms, 3), "learned_order_ms_per_step": round(learned_ms, 3),
+            "gain": round(static_ms / learned_ms - 1.0, 4),
+            "pred_batch_ms": {str(b): round(tm.sched_predict_batch_ms(b), 3) for b in (1024, 16384, 131072)}}
+
+
 def serving(args):
     """Latency under a Poisson load of 1..4096-query requests (C++ driver over
     tm_submit): plain = one request per device batch, continuous = pending
-    requests share batches on two lanes."""
+    requests share batches on two lanes, learned = continuous batching with
+    the learned scheduler's flush points (trained on a calibration load)."""
     from tagmatch_b200 import build
     cmd = [build.SERVE_BENCH, f"filters={args.filters}", "pool=1048576", f"seed={SEED}", f"maxp={MAX_P}",
-           f"rates={args.serve_rates}", "modes=plain,continuous", f"seconds={args.serve_seconds}"]
+           f"rates={args.serve_rates}", f"plain_rates={args.serve_plain_rates}", f"modes={args.serve_modes}",
+           f"seconds={args.serve_seconds}", f"target_ms={args.latency_target_ms}"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
     if out.returncode != 0:
         return {"error": out.stderr[-500:]}
     runs = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
     return {"workload": "Poisson arrivals, request sizes log-uniform 1..4096 queries, 10M-filter table, match",
-            "runs": runs}
+            "runs": runs, "equal_p99": equal_p99(runs)}
+
+
+def equal_p99(runs, levels=(10, 15, 20, 25, 30, 40, 50)):
+    """Sustained queries/s of each mode at equal p99 latency: for each p99
+    level, the highest sustained rate among the mode's runs whose p99 is at
+    or below it (no interpolation), and the ratios to the plain mode."""
+    modes = sorted({r["mode"] for r in runs if "p99_ms" in r})
+    out = []
+    for lv in levels:
+        best = {m: max([r["sustained_qps"] for r in runs if r.get("mode") == m and r["p99_ms"] <= lv], default=None)
+                for m in modes}
+        row = {"p99_ms_at_most": lv, **{m: best[m] for m in modes}}
+        if best.get("plain"):
+            for m in modes:
+                if m != "plain" and best[m]:
+                    row[f"{m}_over_plain"] = round(best[m] / best["plain"], 2)
+        out.append(row)
+    return out
+
+
+def run_config2(args):
+    """The skewed configuration: 100,000,000 filters with Zipf s = 1.3 tags
+    (seed 3; partition sizes from 1 to 65,536, heavily uneven), queries at
+    superset fractions 10%, 50% and 90% (--queries per fraction).  A step is
+    one pass over all three fractions' queries; per fraction: queries/s,
+    keys per query, work items per batch, and the item tail (largest and
+    99th-percentile item warp-cycles over the mean, from one recorded
+    batch).  Tiles per work item and the device batch are autotuned on the
+    50% fraction, the batch capped so that its results fit in memory."""
+    import torch
+    world, rank, local = dist_setup("nccl")
+    torch.cuda.set_device(local)
+    from tagmatch_b200 import TagMatch, workload
+    n_f = args.filters if args.filters != FILTERS else 100_000_000
+    t0 = time.perf_counter()
+    f, ko, k = workload.generate_filters(n_f, 3, zipf_s=1.3)
+    fractions = (0.1, 0.5, 0.9)
+    qs = {s: workload.generate_queries(args.queries, f, 3 + 7919 * rank, zipf_s=1.3, superset_fraction=s)
+          for s in fractions}
+    t_gen = time.perf_counter() - t0
+    tm = TagMatch()
+    tm.set_persistence(False)
+    t0 = time.perf_counter()
+    tm.add_many(f, ko, k)
+    tm.consolidate(MAX_P, 1)
+    t_build = time.perf_counter() - t0
+    info = tm.table_info()
+    stream = torch.cuda.current_stream()
+    dqs = {s: torch.from_numpy(qs[s].view(np.int32)).to("cuda") for s in fractions}
+    nq = args.queries
+    # keys per query on a small sample bound the device batch
+    _, _, nk = tm.match_batch_device(dqs[0.9].data_ptr(), min(nq, 2048), stream=stream.cuda_stream)
+    kpq = max(1.0, nk / min(nq, 2048))
+    cap = int(min(262144, max(1024, 24e9 / (kpq * 9.0))))
+    cap = 1 << (cap.bit_length() - 1)
+    tm.set_batch_limit(cap)
+    tuned = None
+    B = min(args.batch, cap)
+    if args.seg_tiles:
+        tm.set_tiles_per_item(args.seg_tiles)
+    elif not args.no_autotune:
+        seg, bl, tqps = tm.autotune(qs[0.5][: min(nq, cap)])
+        B = min(bl, cap)
+        tuned = {"seg_tiles": seg, "device_batch": bl, "sample_queries_per_s": round(tqps, 1)}
+
+    def step_one(s):
+        keys = 0
+        for b0 in range(0, nq, B):
+            _, _, n = tm.match_batch_device(dqs[s].data_ptr() + b0 * 24, min(B, nq - b0), stream=stream.cuda_stream)
+            keys += n
+        return keys
+
+    for s in fractions:  # warm-up: one device batch per fraction, three times
+        for _ in range(max(3, args.warmup)):
+            tm.match_batch_device(dqs[s].data_ptr(), min(B, nq), stream=stream.cuda_stream)
+    tm.reset_match_stats()
+    tm.set_profiling(True)
+    per = {s: {"ms": 0.0, "keys": 0} for s in fractions}
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            for s in fractions:
+                e0.record(stream)
+                per[s]["keys"] += step_one(s)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                per[s]["ms"] += e0.elapsed_time(e1)
+    tm.set_profiling(False)
+    total_ms = sum(per[s]["ms"] for s in fractions) / args.steps
+    ms_max = max_over_ranks(total_ms, world, device="cuda")
+    st = tm.match_stats()
+    rows = []
+    for s in fractions:
+        tm.sched_record(True)
+        tm.match_batch_device(dqs[s].data_ptr(), min(B, nq), stream=stream.cuda_stream)
+        tm.sched_record(False)
+        _, lc = tm.sched_samples()
+        cyc = np.exp(lc[-max(1, min(lc.size, 1 << 20)):].astype(np.float64)) if lc.size else np.ones(1)
+        rows.append({"superset_fraction": s, "queries_per_s": round(args.steps * nq / (per[s]["ms"] / 1e3), 1),
+                     "ms_per_pass": round(per[s]["ms"] / args.steps, 2),
+                     "keys_per_query": round(per[s]["keys"] / (args.steps * nq), 1),
+                     "items_in_recorded_batch": int(cyc.size),
+                     "item_tail": {"max_over_mean": round(float(cyc.max() / cyc.mean()), 2),
+                                   "p99_over_mean": round(float(np.percentile(cyc, 99) / cyc.mean()), 2)}})
+    launches = max(st["match_kernel_launches"], 1)
+    alg_bytes = (st["dense_tests"] * 24 / 256 + st["routed"] * 24 + st["records"] * 16) / launches
+    kern_s = st["match_kernel_ms"] / 1e3 / launches
+    peak, peak_kind = measured_peaks()
+    line = {"metric": METRIC, "value": round(world * 3 * nq / (ms_max / 1e3), 1), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms_max, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": f"config2: {n_f} filters, Zipf s=1.3 tags (seed 3), {nq} queries per superset "
+                                   f"fraction 10/50/90%, partitions <= {MAX_P}, 256-query partition batches, match",
+                       "filters": n_f, "queries_per_fraction": nq, "device_batch": B, "batch_cap": cap,
+                       "autotuned": tuned, "seg_tiles": tm.get_tiles_per_item(), "partitions": info["partitions"],
+                       "tiles": info["tiles"], "table_device_bytes": info["device_bytes"],
+                       "parallelism": f"replicas x{world}", "build_s": round(t_build, 1), "gen_s": round(t_gen, 1)},
+            "clocks": clk.summary(), "gpu_launches": int(st["kernel_launches"]), "fractions": rows,
+            "roofline": {"bound": "hbm", "achieved": round(alg_bytes / kern_s / 1e9, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(alg_bytes / kern_s / 1e9 / peak, 4), "traffic": None, "peak_source": peak_kind,
+                         "kernel": "k_match (subset test)", "kernel_ms_per_launch": round(kern_s * 1e3, 3),
+                         "alg_bytes_per_launch": int(alg_bytes)}}
+    if rank == 0 and not args.no_parity:
+        par = []
+        for s in fractions:
+            p = parity_check(tm, f, ko, k, qs[s][: min(nq, B)], dqs[s].data_ptr(), B, False, stream.cuda_stream,
+                             max(16, args.parity_samples // 10))
+            par.append({"superset_fraction": s, "checked": p["checked"], "mismatches": p["mismatches"]})
+        line["parity"] = {"checked": sum(p["checked"] for p in par), "mismatches": sum(p["mismatches"] for p in par),
+                          "per_fraction": par, "seg_tiles": tm.get_tiles_per_item(), "device_batch": B}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tm.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def run_ours(args):
@@ -348,6 +527,8 @@ def run_ours(args):
     if rank == 0 and not args.no_parity:
         line["parity"] = parity_check(tm, f, ko, k, q, base, B, args.unique, stream.cuda_stream, args.parity_samples)
         line["parity"].update({"seg_tiles": tm.get_tiles_per_item(), "device_batch": B})
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["learned_scheduler"] = learned_order(tm, step, args, stream)
 
     # ---- end to end through the host C ABI ----
     if not args.no_e2e:
@@ -486,6 +667,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == 2:
+        run_config2(args)
     else:
         run_ours(args)
 

@@ -164,10 +164,18 @@ int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uin
  *   pending requests (up to the batch limit and the memory budget) form the
  *   next batch -- continuous batching;
  * TM_FLUSH_SINGLE: one request per device batch on one lane (the plain
- *   batched path, for comparison). */
+ *   batched path, for comparison);
+ * TM_FLUSH_LEARNED: continuous batching whose flush points come from the
+ *   learned cost model (tm_sched_train): a free lane takes the pending
+ *   requests once they make a batch that keeps up with the measured
+ *   arrival rate (queries over the batch's predicted time >= 1.25 x the
+ *   rate), or once the oldest one's wait plus the batch's predicted time
+ *   reaches half the latency target (tm_set_latency_target_ms); before
+ *   training it behaves as TM_FLUSH_IMMEDIATE. */
 #define TM_FLUSH_FULL_OR_LATENCY 0
 #define TM_FLUSH_IMMEDIATE 1
 #define TM_FLUSH_SINGLE 2
+#define TM_FLUSH_LEARNED 3
 int tm_set_flush_mode(tm_engine *e, int mode);
 /* Device-memory budget per lane for a batch's queues, hit records and keys; the
  * number of queries admitted into one batch is capped by it (estimated
@@ -191,6 +199,48 @@ int tm_balanced_partitioning(const uint32_t *filters, uint64_t n, uint32_t max_p
  * values and the sample's queries/s.  Results do not depend on either. */
 int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg_tiles, uint32_t *batch_limit,
                 double *queries_per_s);
+
+/* Learned scheduler (no reference counterpart; the reference flushes a
+ * partition queue when it is full or older than the latency limit,
+ * front_end.cc:325-376, 563-598).  A cost model, an 8 -> 64 -> 64 -> 1 fp32
+ * MLP trained on the GPU by the library's own kernels, predicts the log of a
+ * subset-test work item's warp-cycles from: partition size, partition mask
+ * popcount, queries queued for the partition, queries in the item, tiles in
+ * the item, recent match density of the partition, filters per tile, tiles
+ * per work item.
+ *
+ * tm_sched_record: while on, every batch the engine matches records its
+ *   work items' timings as samples (features [8] + log warp-cycles).
+ * tm_sched_samples: copies up to capacity samples (features [n][8],
+ *   log_cycles [n]; either may be null) and reports the count in *n.
+ * tm_sched_train: trains the model on all samples (mini-batch Adam, 90/10
+ *   train/validation split), then derives its decisions: the partition
+ *   order of the work queue and the predicted batch times that set the
+ *   learned flush points.  Errors are on standardised log-cycles.
+ * tm_sched_use_order: on = work queue in descending predicted item cost;
+ *   off = partition id order (the static fallback).  Results never depend on
+ *   the order.
+ * tm_sched_predict_batch_ms: predicted device time of a batch of n queries.
+ * tm_set_latency_target_ms: the p99 latency the learned flush points aim
+ *   at (default 25 ms). */
+typedef struct {
+    uint64_t samples, steps;
+    double train_mse, val_mse, val_r2, mean_mse, ms;
+} tm_sched_report;
+int tm_sched_record(tm_engine *e, int on);
+int tm_sched_samples(tm_engine *e, float *features, float *log_cycles, uint64_t capacity, uint64_t *n);
+int tm_sched_train(tm_engine *e, uint32_t epochs, tm_sched_report *report);
+int tm_sched_use_order(tm_engine *e, int on);
+int tm_sched_predict_batch_ms(tm_engine *e, uint32_t queries, double *ms);
+int tm_set_latency_target_ms(tm_engine *e, uint32_t ms);
+/* The cost model's kernels on caller data (for checking them): outputs
+ * [n], the gradient of the mean squared error over the n samples with
+ * respect to all tm_mlp_param_count() parameters (layout: W1 [64][8], b1
+ * [64], W2 [64][64], b2 [64], W3 [64], b3), and the loss.  Runs on the
+ * current CUDA device. */
+uint32_t tm_mlp_param_count(void);
+int tm_mlp_loss_grad(const float *params, const float *features, const float *targets, uint32_t n, float *outputs,
+                     float *grad, float *loss);
 
 /* Tiles per work item of the subset test (what tm_autotune chooses;
  * default 128): each work item is one 256-query chunk of a partition

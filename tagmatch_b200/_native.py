@@ -33,6 +33,7 @@ REQUEST_CALLBACK = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint64, u64p
 TM_FLUSH_FULL_OR_LATENCY = 0
 TM_FLUSH_IMMEDIATE = 1
 TM_FLUSH_SINGLE = 2
+TM_FLUSH_LEARNED = 3
 
 
 class TableInfo(ctypes.Structure):
@@ -48,6 +49,14 @@ class MatchStats(ctypes.Structure):
                 ("kernel_launches", ctypes.c_uint64), ("h2d_bytes", ctypes.c_uint64),
                 ("d2h_bytes", ctypes.c_uint64), ("records", ctypes.c_uint64)]
 
+
+class SchedReport(ctypes.Structure):
+    _fields_ = [("samples", ctypes.c_uint64), ("steps", ctypes.c_uint64), ("train_mse", ctypes.c_double),
+                ("val_mse", ctypes.c_double), ("val_r2", ctypes.c_double), ("mean_mse", ctypes.c_double),
+                ("ms", ctypes.c_double)]
+
+
+f32p = ctypes.POINTER(ctypes.c_float)
 
 # name -> (restype, argtypes); every symbol include/tagmatch_b200.h declares
 SIGNATURES = {
@@ -86,6 +95,14 @@ SIGNATURES = {
     "tm_balanced_partitioning": (ctypes.c_int, [u32p, ctypes.c_uint64, ctypes.c_uint32, u32p, u32p, u32p,
                                                 ctypes.c_uint64, u64p]),
     "tm_autotune": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_uint32, u32p, u32p, ctypes.POINTER(ctypes.c_double)]),
+    "tm_sched_record": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tm_sched_samples": (ctypes.c_int, [ctypes.c_void_p, f32p, f32p, ctypes.c_uint64, u64p]),
+    "tm_sched_train": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(SchedReport)]),
+    "tm_sched_use_order": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tm_sched_predict_batch_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
+    "tm_set_latency_target_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    "tm_mlp_param_count": (ctypes.c_uint32, []),
+    "tm_mlp_loss_grad": (ctypes.c_int, [f32p, f32p, f32p, ctypes.c_uint32, f32p, f32p, f32p]),
     "tm_set_tiles_per_item": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     "tm_get_tiles_per_item": (ctypes.c_uint32, [ctypes.c_void_p]),
     "tm_get_table_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(TableInfo)]),

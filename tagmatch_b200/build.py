@@ -23,8 +23,9 @@ NVCC = os.environ.get("NVCC", "nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["partition.cu", "match.cu", "noalloc.cu", "engine.cu", "capi.cu", "facade.cu"]
-HEADERS = ["tm_device.cuh", "tm_host.hpp", "scan.cuh", "partition.cuh", "match.cuh", "match_kernels.cuh", "engine.cuh"]
+CUDA_SOURCES = ["partition.cu", "match.cu", "noalloc.cu", "sched.cu", "engine.cu", "capi.cu", "facade.cu"]
+HEADERS = ["tm_device.cuh", "tm_host.hpp", "scan.cuh", "partition.cuh", "match.cuh", "match_kernels.cuh", "sched.cuh",
+           "engine.cuh"]
 
 LIB = os.path.join(HERE, "libtagmatch_b200.so")
 WORKLOAD_LIB = os.path.join(HERE, "libtm_workload.so")

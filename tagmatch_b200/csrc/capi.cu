@@ -54,10 +54,7 @@ int tm_add(tm_engine *e, const uint32_t filter[TM_FILTER_WORDS], const uint32_t 
 
 int tm_add_many(tm_engine *e, const uint32_t *filters, uint64_t n, const uint32_t *key_offsets, const uint32_t *keys) {
     if (!e || (n && (!filters || !key_offsets))) return TM_ERR_INVALID;
-    return guard(e, [&] {
-        for (uint64_t i = 0; i < n; ++i)
-            e->eng.add(filters + i * TM_FILTER_WORDS, keys + key_offsets[i], key_offsets[i + 1] - key_offsets[i]);
-    });
+    return guard(e, [&] { e->eng.add_many(filters, n, key_offsets, keys); });
 }
 
 int tm_remove(tm_engine *e, const uint32_t filter[TM_FILTER_WORDS], uint32_t key) {
@@ -162,7 +159,7 @@ int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uin
 }
 
 int tm_set_flush_mode(tm_engine *e, int mode) {
-    if (!e || mode < TM_FLUSH_FULL_OR_LATENCY || mode > TM_FLUSH_SINGLE) return TM_ERR_INVALID;
+    if (!e || mode < TM_FLUSH_FULL_OR_LATENCY || mode > TM_FLUSH_LEARNED) return TM_ERR_INVALID;
     e->eng.set_flush_mode(mode);
     return TM_OK;
 }
@@ -221,6 +218,65 @@ int tm_autotune(tm_engine *e, const uint32_t *queries, uint32_t n, uint32_t *seg
                 double *queries_per_s) {
     if (!e || !queries || n == 0 || !seg_tiles || !batch_limit || !queries_per_s) return TM_ERR_INVALID;
     return guard(e, [&] { e->eng.autotune(queries, n, seg_tiles, batch_limit, queries_per_s); });
+}
+
+int tm_sched_record(tm_engine *e, int on) {
+    if (!e) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.scheduler().set_recording(on != 0); });
+}
+
+int tm_sched_samples(tm_engine *e, float *features, float *log_cycles, uint64_t capacity, uint64_t *n) {
+    if (!e || !n) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.scheduler().export_samples(features, log_cycles, capacity, n); });
+}
+
+int tm_sched_train(tm_engine *e, uint32_t epochs, tm_sched_report *rep) {
+    if (!e || epochs == 0) return TM_ERR_INVALID;
+    return guard(e, [&] {
+        const tmb::TrainReport r = e->eng.train_scheduler(epochs);
+        if (rep) {
+            rep->samples = r.samples;
+            rep->steps = r.steps;
+            rep->train_mse = r.train_mse;
+            rep->val_mse = r.val_mse;
+            rep->val_r2 = r.val_r2;
+            rep->mean_mse = r.mean_mse;
+            rep->ms = r.ms;
+        }
+    });
+}
+
+int tm_sched_use_order(tm_engine *e, int on) {
+    if (!e) return TM_ERR_INVALID;
+    return guard(e, [&] {
+        if (on && !e->eng.scheduler().trained()) throw tmb::Error(TM_ERR_STATE, "the cost model is not trained");
+        e->eng.set_learned_order(on != 0);
+    });
+}
+
+int tm_sched_predict_batch_ms(tm_engine *e, uint32_t queries, double *ms) {
+    if (!e || !ms) return TM_ERR_INVALID;
+    return guard(e, [&] { *ms = e->eng.scheduler().predict_batch_ms(queries); });
+}
+
+int tm_set_latency_target_ms(tm_engine *e, uint32_t ms) {
+    if (!e || ms == 0) return TM_ERR_INVALID;
+    return guard(e, [&] { e->eng.set_latency_target_ms(ms); });
+}
+
+uint32_t tm_mlp_param_count(void) { return uint32_t(tmb::kMlpParams); }
+
+int tm_mlp_loss_grad(const float *params, const float *features, const float *targets, uint32_t n, float *outputs,
+                     float *grad, float *loss) {
+    if (!params || !grad || !loss || (n && (!features || !targets || !outputs))) return TM_ERR_INVALID;
+    try {
+        tmb::CostModel::loss_grad(params, features, targets, n, outputs, grad, loss, nullptr);
+        return TM_OK;
+    } catch (const tmb::Error &x) {
+        return x.status;
+    } catch (...) {
+        return TM_ERR_INTERNAL;
+    }
 }
 
 int tm_set_tiles_per_item(tm_engine *e, uint32_t seg_tiles) {

@@ -102,6 +102,31 @@ bool read_db(const std::string &fn, std::vector<Entry> &out, std::map<FilterKey,
     return true;
 }
 
+// Sorts v with cmp on all hardware threads: sorted chunks, then pairwise
+// merges.
+template <class T, class Cmp>
+void parallel_sort(std::vector<T> &v, Cmp cmp) {
+    const size_t n = v.size();
+    const unsigned th = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n < (size_t(1) << 16) || th == 1) {
+        std::sort(v.begin(), v.end(), cmp);
+        return;
+    }
+    std::vector<size_t> b(th + 1);
+    for (unsigned i = 0; i <= th; ++i) b[i] = n * i / th;
+    std::vector<std::thread> ts;
+    for (unsigned i = 0; i < th; ++i) ts.emplace_back([&, i] { std::sort(v.begin() + b[i], v.begin() + b[i + 1], cmp); });
+    for (auto &t : ts) t.join();
+    for (unsigned w = 1; w < th; w *= 2) {
+        ts.clear();
+        for (unsigned i = 0; i + w < th; i += 2 * w) {
+            const size_t lo = b[i], mid = b[i + w], hi = b[std::min(i + 2 * w, th)];
+            ts.emplace_back([&, lo, mid, hi] { std::inplace_merge(v.begin() + lo, v.begin() + mid, v.begin() + hi, cmp); });
+        }
+        for (auto &t : ts) t.join();
+    }
+}
+
 bool write_db(const std::string &fn, const std::vector<Entry> &fib) {
     std::ofstream out(fn, std::ios::binary | std::ios::trunc);
     if (!out) return false;
@@ -124,6 +149,21 @@ void Engine::consolidate(uint32_t psize, uint32_t threads) {
     if (started_) throw Error(TM_ERR_STATE, "consolidate() while matching: call stop() first");
     partition_size_ = psize;
     partitioning_threads_ = threads;
+    if (!bulk_koff_.empty() && bulk_koff_.size() > 1) {
+        if (!already_consolidated_) {
+            consolidate_bulk();
+            return;
+        }
+        // incremental update: the bulk adds join the staged updates
+        const size_t m = bulk_koff_.size() - 1;
+        for (size_t i = 0; i < m; ++i) {
+            FilterKey f;
+            std::memcpy(f.w.data(), &bulk_words_[i * kWords], 24);
+            KeysetChange &c = updates_[f];
+            for (uint64_t j = bulk_koff_[i]; j < bulk_koff_[i + 1]; ++j) c.to_add.insert(bulk_keys_[j]);
+        }
+        clear_bulk();
+    }
     std::vector<Entry> fib;
     if (already_consolidated_) {
         if (persist_) {
@@ -169,6 +209,118 @@ void Engine::consolidate(uint32_t psize, uint32_t threads) {
     }
     ++table_version_;
     // the partitioner runs at consolidation time, on the first device
+    build_device_table(device(0));
+    already_consolidated_ = true;
+}
+
+void Engine::add_many(const uint32_t *filters, uint64_t n, const uint32_t *key_off, const uint32_t *keys) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (bulk_koff_.empty()) bulk_koff_.push_back(0);
+    bulk_words_.insert(bulk_words_.end(), filters, filters + n * kWords);
+    for (uint64_t i = 0; i < n; ++i) {
+        bulk_keys_.insert(bulk_keys_.end(), keys + key_off[i], keys + key_off[i + 1]);
+        bulk_koff_.push_back(bulk_keys_.size());
+    }
+}
+
+void Engine::clear_bulk() {
+    std::vector<uint32_t>().swap(bulk_words_);
+    std::vector<uint64_t>().swap(bulk_koff_);
+    std::vector<uint32_t>().swap(bulk_keys_);
+}
+
+// First consolidation with bulk adds (tm_add_many): the same table as
+// staging every add in the update map and consolidating it -- filters in
+// bitvector order (bitvector.hh:389-397), each with the ascending union of
+// its keys, empty ones dropped (tagmatch.cc:121-128) -- built by a parallel
+// sort of the bulk entries merged with the map's entries instead of one map
+// insertion per filter.
+void Engine::consolidate_bulk() {
+    struct SortEntry {
+        uint32_t w[kWords];
+        uint32_t idx;
+    };
+    const size_t m = bulk_koff_.size() - 1;
+    std::vector<SortEntry> v(m);
+    for (size_t i = 0; i < m; ++i) {
+        std::memcpy(v[i].w, &bulk_words_[i * kWords], 24);
+        v[i].idx = uint32_t(i);
+    }
+    auto less_words = [](const uint32_t *a, const uint32_t *b) {
+        for (int blk = 0; blk < 3; ++blk) {
+            const uint64_t x = uint64_t(a[2 * blk]) | (uint64_t(a[2 * blk + 1]) << 32);
+            const uint64_t y = uint64_t(b[2 * blk]) | (uint64_t(b[2 * blk + 1]) << 32);
+            if (x != y) return ((y >> __builtin_ctzll(x ^ y)) & 1) != 0;
+        }
+        return false;
+    };
+    // stable in effect: equal filters keep their add order (idx breaks ties)
+    parallel_sort(v, [&](const SortEntry &a, const SortEntry &b) {
+        if (less_words(a.w, b.w)) return true;
+        if (less_words(b.w, a.w)) return false;
+        return a.idx < b.idx;
+    });
+    filters_.clear();
+    key_off_.assign(1, 0);
+    keys_.clear();
+    filters_.reserve(m * kWords);
+    key_off_.reserve(m + 1);
+    keys_.reserve(bulk_keys_.size());
+    std::vector<uint32_t> ks;
+    auto emit = [&](const uint32_t *w, std::vector<uint32_t> &kv) {
+        if (kv.empty()) return;
+        filters_.insert(filters_.end(), w, w + kWords);
+        keys_.insert(keys_.end(), kv.begin(), kv.end());
+        if (keys_.size() >= 0xFFFFFFFFull) throw Error(TM_ERR_INVALID, "table too large (2^32 keys)");
+        key_off_.push_back(uint32_t(keys_.size()));
+    };
+    auto it = updates_.begin();
+    size_t i = 0;
+    while (i < m || it != updates_.end()) {
+        const bool take_map = i == m || (it != updates_.end() && less_words(it->first.w.data(), v[i].w));
+        if (take_map) {
+            ks.clear();
+            it->second.apply(ks);
+            emit(it->first.w.data(), ks);
+            ++it;
+            continue;
+        }
+        // one group of equal filters from the bulk adds
+        size_t j = i;
+        ks.clear();
+        while (j < m && std::memcmp(v[j].w, v[i].w, 24) == 0) {
+            const uint32_t e = v[j].idx;
+            ks.insert(ks.end(), bulk_keys_.begin() + bulk_koff_[e], bulk_keys_.begin() + bulk_koff_[e + 1]);
+            ++j;
+        }
+        if (it != updates_.end() && std::memcmp(it->first.w.data(), v[i].w, 24) == 0) {
+            KeysetChange c = it->second;
+            c.to_add.insert(ks.begin(), ks.end());
+            ks.clear();
+            c.apply(ks);
+            ++it;
+        } else {
+            std::sort(ks.begin(), ks.end());
+            ks.erase(std::unique(ks.begin(), ks.end()), ks.end());
+        }
+        emit(v[i].w, ks);
+        i = j;
+    }
+    updates_.clear();
+    clear_bulk();
+    if (persist_) {
+        std::ofstream out(db_filename_, std::ios::binary | std::ios::trunc);
+        const uint32_t part = 0;
+        for (size_t e = 0; out && e + 1 < key_off_.size(); ++e) {
+            const uint32_t n = key_off_[e + 1] - key_off_[e];
+            out.write(reinterpret_cast<const char *>(&part), 4);
+            out.write(reinterpret_cast<const char *>(&filters_[e * kWords]), 24);
+            out.write(reinterpret_cast<const char *>(&n), 4);
+            out.write(reinterpret_cast<const char *>(&keys_[key_off_[e]]), std::streamsize(n) * 4);
+        }
+        if (!out) std::cerr << "could not open database file: " << db_filename_ << std::endl;
+    }
+    ++table_version_;
     build_device_table(device(0));
     already_consolidated_ = true;
 }
@@ -267,6 +419,7 @@ void Engine::clear() {
     std::lock_guard<std::mutex> lk(api_mtx_);
     already_consolidated_ = false;
     updates_.clear();
+    clear_bulk();
     filters_.clear();
     key_off_.assign(1, 0);
     keys_.clear();
@@ -284,8 +437,18 @@ void Engine::clear() {
 void Engine::enqueue(RequestPtr r) {
     {
         std::lock_guard<std::mutex> ql(q_mtx_);
-        if (pending_.empty()) oldest_ = std::chrono::steady_clock::now();
+        r->arrived = std::chrono::steady_clock::now();
+        if (pending_.empty()) oldest_ = r->arrived;
         pending_queries_ += r->n;
+        // arrival rate (queries/s), smoothed over windows of >= 10 ms
+        arrived_queries_ += r->n;
+        const double dt = std::chrono::duration<double>(r->arrived - rate_t_).count();
+        if (dt >= 0.01) {
+            const double sample = double(arrived_queries_ - rate_q_) / dt;
+            arrival_qps_ = dt > 1.0 ? sample : 0.5 * arrival_qps_ + 0.5 * sample;
+            rate_t_ = r->arrived;
+            rate_q_ = arrived_queries_;
+        }
         pending_.push_back(std::move(r));
     }
     q_cv_.notify_all();
@@ -341,6 +504,28 @@ void Engine::worker_loop(int dev, int lane) {
                     continue;
                 }
                 if (!pending_.empty()) {
+                    if (mode == kFlushLearned && !stopping_ && !flush_now_ && pending_queries_ < batch_limit_ &&
+                        sched_.trained()) {
+                        // learned flush point: go when the pending queries make a
+                        // batch large enough to keep up with the arrival rate
+                        // (predicted queries per ms of batch time), or when the
+                        // oldest request's wait plus the batch's predicted time
+                        // reaches half the latency target; otherwise wait for
+                        // more requests
+                        const uint64_t bq = std::max<uint64_t>(1, memory_budget_.load() / std::max<uint64_t>(1, bytes_per_query_.load()));
+                        const uint32_t cap = uint32_t(std::min<uint64_t>(batch_limit_, bq));
+                        const uint32_t b0 = uint32_t(std::min<uint64_t>(pending_queries_, cap));
+                        const double t0 = sched_.predict_batch_ms(b0);
+                        const auto now = std::chrono::steady_clock::now();
+                        const double age = std::chrono::duration<double, std::milli>(now - pending_.front()->arrived).count();
+                        const double budget = 0.5 * latency_target_ms_.load();
+                        const uint32_t need = sched_.stable_batch(arrival_qps_, cap);
+                        if (b0 >= need || age + t0 >= budget) break;
+                        double wait_ms = budget - age - t0;
+                        if (arrival_qps_ > 0) wait_ms = std::min(wait_ms, 1e3 * double(need - b0) / arrival_qps_);
+                        q_cv_.wait_until(lk, now + std::chrono::microseconds(int64_t(1e3 * wait_ms) + 1));
+                        continue;
+                    }
                     if (stopping_ || flush_now_ || mode != kFlushFullOrLatency || pending_queries_ >= batch_limit_) break;
                     const uint32_t lim = latency_ms_.load();
                     if (lim > 0) {
@@ -403,7 +588,11 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
         const uint32_t *dkeys;
         uint64_t nk = 0;
         BatchStats bs;
+        prepare(ln.scratch);
+        const auto tb = std::chrono::steady_clock::now();
         match_batch(d.table, ln.scratch.queries.p, nq, unique, ln.scratch, &doff, &dkeys, &nk, &bs, ln.stream);
+        observe(d.table, ln.scratch, nq, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count(),
+                nk);
         ln.h_offsets.reserve(size_t(nq) + 1);
         ln.h_keys.reserve(std::max<uint64_t>(nk, 1));
         TM_CUDA(cudaMemcpyAsync(ln.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, ln.stream));
@@ -473,7 +662,11 @@ void Engine::match_device(const uint32_t *d_queries, uint32_t nq, bool unique, c
     TM_CUDA(cudaSetDevice(d.id));
     BatchStats local;
     d.scratch.profile = profile_;
+    prepare(d.scratch);
+    const auto tb = std::chrono::steady_clock::now();
     match_batch(d.table, d_queries, nq, unique, d.scratch, d_offsets, d_keys, n_keys, &local, st ? st : d.stream, ev0, ev1);
+    observe(d.table, d.scratch, nq, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count(),
+            *n_keys);
     stats_.add(local, nq, profile_);
     if (bs) *bs = local;
 }
@@ -503,6 +696,8 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     cudaEvent_t e0, e1;
     TM_CUDA(cudaEventCreate(&e0));
     TM_CUDA(cudaEventCreate(&e1));
+    d.scratch.record_items = false;  // the candidates' batches are timed, not recorded
+    d.scratch.part_order.clear();
     double best = -1.0;
     uint32_t best_seg = seg_tiles_, best_batch = batch_limit_;
     const uint32_t segs[] = {32, 64, 128, 256, 512, 1024, 2048, 4096, 8192};
@@ -547,6 +742,28 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     *seg_out = best_seg;
     *batch_out = best_batch;
     *qps_out = best;
+}
+
+void Engine::prepare(MatchScratch &s) {
+    s.record_items = sched_.recording();
+    if (learned_order_.load()) s.part_order = sched_.order();
+    else s.part_order.clear();
+}
+
+void Engine::observe(const DevTable &t, const MatchScratch &s, uint32_t nq, double ms, uint64_t keys) {
+    if (s.record_items) sched_.absorb(t, s, nq, ms, keys);
+}
+
+TrainReport Engine::train_scheduler(uint32_t epochs) {
+    std::lock_guard<std::mutex> lk(api_mtx_);
+    if (!already_consolidated_) throw Error(TM_ERR_STATE, "train the scheduler after consolidate()");
+    Device &d = device(0);
+    if (dev_version_[0] != table_version_) build_device_table(d);
+    TM_CUDA(cudaSetDevice(d.id));
+    int sms = 0, khz = 0;
+    TM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.id));
+    TM_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, d.id));
+    return sched_.train(d.table, seg_tiles_, sms, double(khz) * 1e3, epochs, d.stream);
 }
 
 void Engine::apply_seg_tiles(uint32_t seg) {
@@ -767,7 +984,9 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             uint64_t nk = 0;
             BatchStats bs;
             sc.profile = profile_;
+            prepare(sc);
             match_batch(d.table, sc.queries.p, n, unique, sc, &doff, &dkeys, &nk, &bs, str[l]);
+            observe(d.table, sc, n, std::chrono::duration<double, std::milli>(TClock::now() - t_begin).count(), nk);
             stats_.add(bs, n, profile_);
             stats_.h2d_bytes += uint64_t(n) * 24;
             h.h_offsets.reserve(size_t(n) + 1);

@@ -3,6 +3,7 @@
 #pragma once
 #include <array>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
@@ -14,6 +15,7 @@
 #include <thread>
 #include <vector>
 #include "match.cuh"
+#include "sched.cuh"
 
 namespace tmb {
 
@@ -67,6 +69,7 @@ struct Request {
     BatchCallback bcb = nullptr;
     void *user = nullptr;
     uint32_t taken = 0;  // queries placed in device batches (queue lock)
+    std::chrono::steady_clock::time_point arrived;  // when it was queued
     // pieces of a request split over several device batches
     std::mutex mtx;
     uint32_t done = 0;
@@ -81,6 +84,7 @@ enum FlushMode : int {
     kFlushFullOrLatency = 0,  // full batch, latency limit, or stop() (front_end.cc semantics)
     kFlushImmediate = 1,      // whenever a lane is free: continuous batching of all pending requests
     kFlushSingle = 2,         // one request per device batch, one lane (plain batched path)
+    kFlushLearned = 3,        // continuous batching with flush points from the learned cost model
 };
 
 struct EngineStats {
@@ -115,6 +119,9 @@ public:
 
     // staging (tagmatch.cc:62-77)
     void add(const uint32_t *filter, const uint32_t *keys, uint32_t n);
+    // n filters [n][6] with keys in CSR form; staged in bulk arrays and
+    // merged at consolidate (same table as n calls of add)
+    void add_many(const uint32_t *filters, uint64_t n, const uint32_t *key_off, const uint32_t *keys);
     void remove(const uint32_t *filter, uint32_t key);
     void set_db(const std::string &f) { db_filename_ = f; }
     const std::string &db() const { return db_filename_; }
@@ -170,6 +177,11 @@ public:
     void set_seg_tiles(uint32_t seg);
     uint32_t seg_tiles() const { return seg_tiles_; }
     bool profiling() const { return profile_; }
+    // learned scheduler (sched.cuh)
+    Scheduler &scheduler() { return sched_; }
+    TrainReport train_scheduler(uint32_t epochs);
+    void set_learned_order(bool on) { learned_order_.store(on); }
+    void set_latency_target_ms(uint32_t ms) { latency_target_ms_.store(ms ? ms : 1); }
     bool started() const { return started_; }
     // host copy of the consolidated filters (table order) and keys
     const std::vector<uint32_t> &filters() const { return filters_; }
@@ -215,13 +227,22 @@ private:
         Lane lanes[kLanes];         // asynchronous matcher lanes
     };
     void build_device_table(Device &d);
+    // before / after every batch: work-queue order and timing record
+    void prepare(MatchScratch &s);
+    void observe(const DevTable &t, const MatchScratch &s, uint32_t nq, double ms, uint64_t keys);
     void apply_seg_tiles(uint32_t seg);
+    void consolidate_bulk();
+    void clear_bulk();
     Device &device(int i);
     void enqueue(RequestPtr r);
     void worker_loop(int dev, int lane);
     void run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool unique);
 
     std::map<FilterKey, KeysetChange> updates_;
+    // bulk adds since the last consolidate: filters [m][6], key offsets [m + 1], keys
+    std::vector<uint32_t> bulk_words_;
+    std::vector<uint64_t> bulk_koff_;
+    std::vector<uint32_t> bulk_keys_;
     bool already_consolidated_ = false;
     bool persist_ = true;
     std::string db_filename_ = "tagmatch.db";
@@ -256,6 +277,14 @@ private:
     uint64_t in_flight_ = 0;
     bool started_ = false, stopping_ = false, flush_now_ = false;
     std::string async_error_;
+
+    Scheduler sched_;
+    std::atomic<bool> learned_order_{false};
+    std::atomic<uint32_t> latency_target_ms_{25};
+    // arrival rate of asynchronous queries (queue lock)
+    uint64_t arrived_queries_ = 0, rate_q_ = 0;
+    std::chrono::steady_clock::time_point rate_t_{};
+    double arrival_qps_ = 0;
 };
 
 }  // namespace tmb

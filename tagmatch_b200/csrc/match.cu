@@ -15,8 +15,10 @@
 //                shared memory); CTA-local counts reserve queue space with
 //                one global atomic per (CTA, partition); queue records are
 //                32 bytes (6 query words, query id, pad);
-//   host plan    work items = (partition, 256-query chunk, 128-tile segment),
-//                offsets computed on the host from the per-partition counts;
+//   host plan    work items = (partition, 256-query chunk, segment of the
+//                partition's tiles), offsets computed on the host from the
+//                per-partition counts, partitions in id order or in the
+//                order the learned cost model gives;
 //   k_slices     per 256-query chunk, bit-sliced "lacks bit b" masks:
 //                Z[b] bit j set when query j of the chunk lacks bit b
 //                (192 x 256 bits, ballot per bit);
@@ -25,9 +27,10 @@
 //                bulk TMA copies (cp.async.bulk + mbarrier), double-buffered:
 //                the next item loads while this one is matched, and the
 //                buffer is released by per-warp mbarrier arrivals instead of
-//                a CTA barrier.  Each warp takes one tile of <= 32 filters;
-//                the tile's AND mask selects candidate queries by OR-ing the
-//                slices of its bits (8 lanes, one 32-query word each); the
+//                a CTA barrier.  Each warp takes four tiles of <= 32 filters;
+//                each tile's AND mask selects candidate queries by OR-ing the
+//                slices of its bits (8 lanes per tile, one 32-query word
+//                each); the
 //                candidates are tested either one per lane against the
 //                tile's filters broadcast from shared memory, or, when they
 //                are few, four at a time against the tile held one filter
@@ -72,6 +75,11 @@ MatchScratch &MatchScratch::operator=(MatchScratch &&o) noexcept {
     uoff = std::move(o.uoff);
     ukeys = std::move(o.ukeys);
     readback = std::move(o.readback);
+    part_order = std::move(o.part_order);
+    d_part_order = std::move(o.d_part_order);
+    record_items = o.record_items;
+    item_stats = std::move(o.item_stats);
+    h_item_stats = std::move(o.h_item_stats);
     for (int i = 0; i < 2 * ScanScratch::kLevels; ++i) scr.levels[i] = std::move(o.scr.levels[i]);
     sm_count = o.sm_count;
     rec_cap_hint = o.rec_cap_hint;
@@ -187,14 +195,24 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     uint32_t chunks = 0, items = 0;
     for (uint32_t p = 0; p < P; ++p) {
         s.h_chunk_off[p] = chunks;
-        s.h_item_off[p] = items;
+        chunks += (s.h_part_count[p] + kChunk - 1) / kChunk;
+    }
+    // work items in the queue order: partition id order, or the order the
+    // learned cost model gives (most expensive items first)
+    const bool ordered = s.part_order.size() == P;
+    for (uint32_t pos = 0; pos < P; ++pos) {
+        const uint32_t p = ordered ? s.part_order[pos] : pos;
+        s.h_item_off[pos] = items;
         const uint32_t nc = (s.h_part_count[p] + kChunk - 1) / kChunk;
         const uint32_t nt = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
-        chunks += nc;
         items += nc * ((nt + s.seg_tiles - 1) / s.seg_tiles);
     }
     s.h_chunk_off[P] = chunks;
     s.h_item_off[P] = items;
+    if (ordered) {
+        s.d_part_order.reserve(P);
+        TM_CUDA(cudaMemcpyAsync(s.d_part_order.p, s.part_order.data(), size_t(P) * 4, cudaMemcpyHostToDevice, st));
+    }
     s.item_off.reserve(size_t(P) + 1);
     s.chunk_off.reserve(size_t(P) + 1);
     TM_CUDA(cudaMemcpyAsync(s.item_off.p, s.h_item_off.data(), (size_t(P) + 1) * 4, cudaMemcpyHostToDevice, st));
@@ -218,9 +236,14 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         }
         // per-query key totals are summed by the subset test itself
         TM_CUDA(cudaMemsetAsync(s.qkeys.p, 0, nq * sizeof(uint32_t), st));
+        if (s.record_items) {
+            s.item_stats.reserve(2 * size_t(std::max<uint32_t>(items, 1)));
+            TM_CUDA(cudaMemsetAsync(s.item_stats.p, 0, 2 * size_t(items) * sizeof(unsigned long long), st));
+        }
         MatchArgs a{t.tile_words.p, t.tile_info.p, t.tile_keys.p, t.slot_key_off.p, t.part_tile_begin.p, s.part_count.p,
                     s.part_off.p, s.item_off.p, s.chunk_off.p, s.queue.p, s.slices.p, P, s.seg_tiles, s.counters.p,
                     s.recs.p, (unsigned long long)s.recs.cap, s.qkeys.p, fpl_trip_cost(),
+                    ordered ? s.d_part_order.p : nullptr, s.record_items ? s.item_stats.p : nullptr,
                     work_counters ? s.work.p : nullptr};
         if (match_begin && attempt == 0) TM_CUDA(cudaEventRecord(match_begin, st));
         if (s.profile) {
@@ -257,6 +280,12 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
         bs.retries++;
     }
     bs.records = hc[1];
+    if (s.record_items) {
+        s.h_item_stats.resize(2 * size_t(items));
+        if (items)
+            TM_CUDA(cudaMemcpyAsync(s.h_item_stats.data(), s.item_stats.p, 2 * size_t(items) * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st));
+    }
     // ---- keys ----
     const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256 * kFillPerLane), unsigned(s.sm_count) * 16));
     // record-count readback, fill, key-total readback; each retry: match + readback

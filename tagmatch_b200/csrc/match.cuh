@@ -31,6 +31,15 @@ struct MatchScratch {
     DevBuf<uint32_t> ukeys;       // [total unique] (also radix temp)
     MappedBuf<uint32_t> readback; // small device results read by the host (k_readback)
     std::vector<uint32_t> h_part_count, h_chunk_off, h_item_off;
+    // work-queue order of the partitions (empty: id order); set by the
+    // engine from the learned cost model
+    std::vector<uint32_t> part_order;
+    DevBuf<uint32_t> d_part_order;
+    // per-item timing record of the subset test (for the cost model):
+    // [2 item] warp-cycles, [2 item + 1] hit records, item = queue position
+    bool record_items = false;
+    DevBuf<unsigned long long> item_stats;
+    std::vector<unsigned long long> h_item_stats;
     ScanScratch scr;
     int sm_count = 0;
     size_t rec_cap_hint = 0;

@@ -202,6 +202,12 @@ struct MatchArgs {
     unsigned long long rec_cap;
     uint32_t *qkeys;               // [batch queries] key totals, zeroed by the caller
     uint32_t fpl_trip_cost;        // path choice: estimated cost of one 4-candidate trip of the lane-per-filter loop
+    // work-queue order: item_off runs over positions, part_order[pos] is the
+    // partition at that position (null: partition id order)
+    const uint32_t *part_order;
+    // optional timing record per item: [2 item] warp-cycles summed over the
+    // CTA's warps, [2 item + 1] hit records; null when off
+    unsigned long long *item_stats;
     // optional work counters (diagnostics): [0] tile visits, [1] passes of
     // the lane-per-query path, [2] candidate (query, tile) pairs, [3] trips
     // of the lane-per-filter path, [4] items, [5] 4-filter groups tested by
@@ -260,9 +266,10 @@ __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
         if (a.item_off[mid] <= item) lo = mid;
         else hi = mid;
     }
+    const uint32_t local = item - a.item_off[lo];
+    if (a.part_order) lo = a.part_order[lo];
     ItemRef r;
     r.p = lo;
-    const uint32_t local = item - a.item_off[lo];
     const uint32_t pq = a.part_count[lo];
     const uint32_t nchunks = (pq + kChunk - 1) / kChunk;
     const uint32_t chunk = local % nchunks, seg = local / nchunks;
@@ -316,7 +323,9 @@ __device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, Matc
 //    added to qkeys[query] (for the prefix sum that places its keys).
 // The path per tile is chosen from the candidate count and the tile size
 // (estimated instruction costs; the choice does not change results).
-template <bool COUNT>
+// COUNT: diagnostics instantiation that also tallies its work (a.work);
+// TIMED: records each item's warp-cycles and hit records (a.item_stats).
+template <bool COUNT, bool TIMED>
 __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4 CTAs per SM: up to 64 registers
     extern __shared__ __align__(128) unsigned char smem_raw[];
     MatchSmem &S = *reinterpret_cast<MatchSmem *>(smem_raw);
@@ -342,7 +351,8 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
         S.inflight_par = 0;
     }
     uint32_t w_tiles = 0, w_passes = 0, w_cand = 0, w_trips = 0, w_items = 0, w_groups = 0;
-    uint32_t wn = 0;     // records staged by this warp (warp-uniform)
+    uint32_t wn = 0;      // records staged by this warp (warp-uniform)
+    uint32_t w_recs = 0;  // records this warp has produced (warp-uniform)
     uint32_t pairs = 0;  // matching (query, filter) pairs found by this lane
     const uint32_t lane_lt = (1u << lane) - 1u;
     uint32_t *tfw = reinterpret_cast<uint32_t *>(S.tf[warp]);
@@ -373,6 +383,12 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
         if (__any_sync(kFull, item >= total || S.fail)) break;
         const ItemRef r = locate(a, item);
         if (COUNT) ++w_items;
+        long long item_c0 = 0;
+        uint32_t item_recs0 = 0;
+        if (TIMED) {
+            item_c0 = clock64();
+            item_recs0 = w_recs;
+        }
         const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[b].q);
         const uint32_t *sz = S.st[b].z;
         for (uint32_t t0 = r.tb + warp * kQuad; t0 < r.te; t0 += kMatchWarps * kQuad) {
@@ -487,6 +503,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                             pairs += __popc(m);
                         }
                         wn += __popc(wm);
+                        if (TIMED) w_recs += __popc(wm);
                     }
                 } else {
                     const bool lane_valid = lane < count;
@@ -545,6 +562,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                             pairs += __popc(mine);
                         }
                         wn += __popc(wm);
+                        if (TIMED) w_recs += __popc(wm);
                     }
                 }
                 __syncwarp();  // the tile buffer is rebuilt for the next tile
@@ -552,6 +570,10 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
             __syncwarp();  // the lists are rebuilt for the next four tiles
         }
         __syncwarp();
+        if (TIMED && lane == 0) {
+            atomicAdd(&a.item_stats[2 * size_t(item)], (unsigned long long)(clock64() - item_c0));
+            atomicAdd(&a.item_stats[2 * size_t(item) + 1], (unsigned long long)(w_recs - item_recs0));
+        }
         if (lane == 0) mbar_arrive(&S.empty[b]);
     }
     if (wn) flush_recs(S.rec[warp], wn, a, lane);
@@ -576,12 +598,19 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
 
 // Launches the subset test on grid CTAs (its shared memory is above the
 // 48 KB static limit, so the size is set on the kernel first).
+template <bool COUNT, bool TIMED>
+inline void launch_match_t(const MatchArgs &a, unsigned grid, cudaStream_t st) {
+    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT, TIMED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(MatchSmem))));
+    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT, TIMED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared)));
+    k_match<COUNT, TIMED><<<grid, kMatchThreads, sizeof(MatchSmem), st>>>(a);
+}
+
 template <bool COUNT>
 inline void launch_match(const MatchArgs &a, unsigned grid, cudaStream_t st) {
-    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(MatchSmem))));
-    TM_CUDA(cudaFuncSetAttribute(k_match<COUNT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 int(cudaSharedmemCarveoutMaxShared)));
-    k_match<COUNT><<<grid, kMatchThreads, sizeof(MatchSmem), st>>>(a);
+    if (a.item_stats) launch_match_t<COUNT, true>(a, grid, st);
+    else launch_match_t<COUNT, false>(a, grid, st);
 }
 
 // ---------------------------------------------------------------------------

@@ -194,7 +194,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     HitRec *recs = ar.take<HitRec>(rec_room - 32, "hit records");
     MatchArgs a{t.tile_words.p, t.tile_info.p, t.tile_keys.p, t.slot_key_off.p, t.part_tile_begin.p, part_count, part_off,
                 item_off, chunk_off, queue, slices, P, seg_tiles, counters, recs, (unsigned long long)(rec_room - 32), qkeys,
-                fpl_trip_cost(), nullptr};
+                fpl_trip_cost(), nullptr, nullptr, nullptr};
     launch_match<false>(a, unsigned(sms) * 4, st);
     TM_CHECK_LAUNCH();
     unsigned long long hc[3] = {0, 0, 0};

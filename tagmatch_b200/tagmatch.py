@@ -247,6 +247,39 @@ class TagMatch:
                                           ctypes.byref(qps)))
         return seg.value, bl.value, qps.value
 
+    # -- learned scheduler ---------------------------------------------------
+    def sched_record(self, on):
+        """Record per-work-item timings of every batch as cost-model samples."""
+        self._check(self._lib.tm_sched_record(self._h, 1 if on else 0))
+
+    def sched_samples(self):
+        """Returns (features [n, 8] float32, log warp-cycles [n] float32)."""
+        n = ctypes.c_uint64(0)
+        self._check(self._lib.tm_sched_samples(self._h, None, None, 0, ctypes.byref(n)))
+        x = np.zeros((n.value, 8), dtype=np.float32)
+        t = np.zeros(n.value, dtype=np.float32)
+        f32 = ctypes.POINTER(ctypes.c_float)
+        self._check(self._lib.tm_sched_samples(self._h, x.ctypes.data_as(f32), t.ctypes.data_as(f32), n.value,
+                                               ctypes.byref(n)))
+        return x, t
+
+    def sched_train(self, epochs=20):
+        """Trains the cost model on the GPU; returns its report as a dict."""
+        rep = _native.SchedReport()
+        self._check(self._lib.tm_sched_train(self._h, epochs, ctypes.byref(rep)))
+        return {k: getattr(rep, k) for k, _ in rep._fields_}
+
+    def sched_use_order(self, on):
+        self._check(self._lib.tm_sched_use_order(self._h, 1 if on else 0))
+
+    def sched_predict_batch_ms(self, queries):
+        ms = ctypes.c_double(0)
+        self._check(self._lib.tm_sched_predict_batch_ms(self._h, queries, ctypes.byref(ms)))
+        return ms.value
+
+    def set_latency_target_ms(self, ms):
+        self._check(self._lib.tm_set_latency_target_ms(self._h, ms))
+
     def set_tiles_per_item(self, seg_tiles):
         """Tiles per work item of the subset test (the autotuner's knob)."""
         self._check(self._lib.tm_set_tiles_per_item(self._h, seg_tiles))
@@ -304,6 +337,25 @@ def read_device(ptr, count, dtype):
         if st != 0:
             raise TagMatchError(_native.TM_ERR_CUDA, f"cudaMemcpy device->host failed ({st})")
     return out
+
+
+def mlp_loss_grad(params, features, targets):
+    """The cost model's GPU kernels on given data: (outputs [n], gradient of
+    the mean squared error [P], loss)."""
+    lib = load()
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 8)
+    t = np.ascontiguousarray(targets, dtype=np.float32)
+    n = x.shape[0]
+    y = np.zeros(max(n, 1), dtype=np.float32)
+    g = np.zeros(p.size, dtype=np.float32)
+    loss = ctypes.c_float(0)
+    f32 = ctypes.POINTER(ctypes.c_float)
+    st = lib.tm_mlp_loss_grad(p.ctypes.data_as(f32), x.ctypes.data_as(f32), t.ctypes.data_as(f32), n,
+                              y.ctypes.data_as(f32), g.ctypes.data_as(f32), ctypes.byref(loss))
+    if st != _native.TM_OK:
+        raise TagMatchError(st, "tm_mlp_loss_grad failed")
+    return y[:n], g, loss.value
 
 
 def balanced_partitioning(filters, max_p):

@@ -365,6 +365,79 @@ def test_serve_bench_runs():
         assert l["requests"] > 0 and l["p99_ms"] >= l["p50_ms"] > 0
 
 
+def test_bulk_add_same_table_as_single_adds(tmp_path):
+    """tm_add_many (sorted bulk merge at the first consolidate) builds the
+    same table as one tm_add per filter (the staged update map,
+    tagmatch.cc:22-34, 98-165): duplicated filters merge their keys, staged
+    single adds and removals combine with the bulk ones.  The database files
+    (table order, keys per filter) are byte-identical and so are the
+    matches."""
+    f, ko, k = workload.generate_filters(30000, 71)
+    r = np.random.default_rng(4)
+    dup = r.choice(f.shape[0], 3000, replace=False)
+    f2 = np.concatenate([f, f[dup]])
+    extra = r.integers(0, 65536, size=3000, dtype=np.uint32)
+    ko2 = np.concatenate([ko, ko[-1] + np.arange(1, 3001, dtype=np.uint32)])
+    k2 = np.concatenate([k, extra])
+    singles = [(f[i], int(r.integers(0, 65536))) for i in r.choice(f.shape[0], 500, replace=False)]
+    removes = [(f[i], int(k[ko[i]])) for i in r.choice(f.shape[0], 300, replace=False)]
+    q = workload.generate_queries(2000, f, 71)
+    dbs, res = [], []
+    for bulk in (False, True):
+        tm = TagMatch()
+        db = str(tmp_path / f"bulk{int(bulk)}.db")
+        tm.set_database_filename(db)
+        if bulk:
+            tm.add_many(f2, ko2, k2)
+        else:
+            for i in range(f2.shape[0]):
+                tm.add(f2[i], k2[ko2[i]:ko2[i + 1]])
+        for w, key in singles:
+            tm.add(w, [key])
+        for w, key in removes:
+            tm.remove(w, key)
+        tm.consolidate(4096, 1)
+        res.append(tm.match_batch(q))
+        tm.close()
+        dbs.append(open(db, "rb").read())
+    assert dbs[0] == dbs[1]
+    assert_same_multisets(res[0][0], res[0][1], res[1][0], res[1][1])
+
+
+@pytest.mark.parametrize("seg_tiles", [128, 4096])
+def test_config2_skewed_table_sampled_parity(seg_tiles):
+    """The skewed configuration at a tenth of its size: 10,000,000 filters
+    with Zipf s = 1.3 tags (seed 3), so partition sizes are heavily uneven,
+    and 4,096 queries at superset fractions 10%, 50% and 90%.  Every 64th
+    query's keys are read back from the device and compared, as (count,
+    multiset hash), with the oracle's single pass over the table; its
+    match_unique keys must be the sorted de-duplicated match keys."""
+    import torch
+    from tagmatch_b200.tagmatch import read_device
+    f, ko, k = workload.generate_filters(10_000_000, 3, zipf_s=1.3)
+    tm = engine_with(f, ko, k, 65536)
+    tm.set_tiles_per_item(seg_tiles)
+    info = tm.table_info()
+    assert info["partitions"] >= 10_000_000 // 65536
+    for sup in (0.1, 0.5, 0.9):
+        q = workload.generate_queries(4096, f, 3, zipf_s=1.3, superset_fraction=sup)
+        sel = np.arange(0, 4096, 64)
+        ec, eh = oracle.match_digest(f, ko, k, q[sel])
+        dq = torch.from_numpy(q.view(np.int32)).cuda()
+        torch.cuda.synchronize()
+        got = {}
+        for unique in (False, True):
+            po, pk, nk = tm.match_batch_device(dq.data_ptr(), q.shape[0], unique=unique)
+            off = read_device(po, q.shape[0] + 1, np.uint64)
+            assert int(off[-1]) == nk
+            got[unique] = [read_device(pk + int(off[i]) * 4, int(off[i + 1] - off[i]), np.uint32) for i in sel]
+        for j in range(sel.size):
+            c, h = oracle.digest(np.array([0, got[False][j].size], dtype=np.uint64), got[False][j])
+            assert c[0] == ec[j] and h[0] == eh[j], (sup, int(sel[j]))
+            assert np.array_equal(np.unique(got[False][j]), got[True][j])
+    tm.close()
+
+
 @pytest.mark.skipif(not os.environ.get("TM_SCALE_TEST"), reason="set TM_SCALE_TEST=1: 100M-filter table (minutes)")
 def test_config2_scale_sampled_parity():
     """100,000,000 filters (Zipf s=1.3, seed 3): the GPU partitioner and
