@@ -66,12 +66,13 @@ def parse():
     ap.add_argument("--parity-samples", type=int, default=2000)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-rates", default="250000,500000,650000,800000,1000000,2000000")
-    ap.add_argument("--serve-plain-rates", default="100000,150000,200000,300000,450000")
+    ap.add_argument("--serve-rates", default="250000,500000,750000,1000000,1500000")
+    ap.add_argument("--serve-plain-rates", default="100000,150000,200000,300000")
     ap.add_argument("--serve-modes", default="plain,continuous,learned")
+    ap.add_argument("--serve-results", default="host,device")
     ap.add_argument("--latency-target-ms", type=int, default=25)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned work-queue order comparison")
-    ap.add_argument("--serve-seconds", type=float, default=4.0)
+    ap.add_argument("--serve-seconds", type=float, default=3.0)
     return ap.parse_args()
 
 
@@ -272,13 +273,16 @@ def serving(args):
     from tagmatch_b200 import build
     cmd = [build.SERVE_BENCH, f"filters={args.filters}", "pool=1048576", f"seed={SEED}", f"maxp={MAX_P}",
            f"rates={args.serve_rates}", f"plain_rates={args.serve_plain_rates}", f"modes={args.serve_modes}",
-           f"seconds={args.serve_seconds}", f"target_ms={args.latency_target_ms}"]
+           f"seconds={args.serve_seconds}", f"target_ms={args.latency_target_ms}", f"results={args.serve_results}"]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
     if out.returncode != 0:
         return {"error": out.stderr[-500:]}
     runs = [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
-    return {"workload": "Poisson arrivals, request sizes log-uniform 1..4096 queries, 10M-filter table, match",
-            "runs": runs, "equal_p99": equal_p99(runs)}
+    return {"workload": "Poisson arrivals, request sizes log-uniform 1..4096 queries, 10M-filter table, match; "
+                        "results copied to host memory (host) or left in device memory (device)",
+            "runs": runs,
+            "equal_p99": {res: equal_p99([r for r in runs if r.get("results") == res])
+                          for res in args.serve_results.split(",")}}
 
 
 def equal_p99(runs, levels=(10, 15, 20, 25, 30, 40, 50)):

@@ -177,6 +177,17 @@ int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uin
 #define TM_FLUSH_SINGLE 2
 #define TM_FLUSH_LEARNED 3
 int tm_set_flush_mode(tm_engine *e, int mode);
+/* Where tm_submit's results go (no reference counterpart; the reference
+ * always returns keys to the host, back_end.cc:288-302):
+ * TM_RESULTS_HOST (default): offsets and keys in host memory;
+ * TM_RESULTS_DEVICE: offsets in host memory, keys left in device memory --
+ *   the callback's keys argument is a device pointer on the engine's first
+ *   device, valid only until the callback returns (copy or consume it
+ *   before returning).  Only whole requests with a request callback; a
+ *   request split over batches still gets host keys. */
+#define TM_RESULTS_HOST 0
+#define TM_RESULTS_DEVICE 1
+int tm_set_serving_results(tm_engine *e, int where);
 /* Device-memory budget per lane for a batch's queues, hit records and keys; the
  * number of queries admitted into one batch is capped by it (estimated
  * from the bytes per query of recent batches).  Default 16 GiB. */

@@ -34,6 +34,8 @@ TM_FLUSH_FULL_OR_LATENCY = 0
 TM_FLUSH_IMMEDIATE = 1
 TM_FLUSH_SINGLE = 2
 TM_FLUSH_LEARNED = 3
+TM_RESULTS_HOST = 0
+TM_RESULTS_DEVICE = 1
 
 
 class TableInfo(ctypes.Structure):
@@ -91,6 +93,7 @@ SIGNATURES = {
     "tm_submit": (ctypes.c_int, [ctypes.c_void_p, u32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, REQUEST_CALLBACK,
                                  ctypes.c_void_p]),
     "tm_set_flush_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "tm_set_serving_results": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "tm_set_memory_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "tm_balanced_partitioning": (ctypes.c_int, [u32p, ctypes.c_uint64, ctypes.c_uint32, u32p, u32p, u32p,
                                                 ctypes.c_uint64, u64p]),

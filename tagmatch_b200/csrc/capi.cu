@@ -164,6 +164,12 @@ int tm_set_flush_mode(tm_engine *e, int mode) {
     return TM_OK;
 }
 
+int tm_set_serving_results(tm_engine *e, int where) {
+    if (!e || (where != TM_RESULTS_HOST && where != TM_RESULTS_DEVICE)) return TM_ERR_INVALID;
+    e->eng.set_device_results(where == TM_RESULTS_DEVICE);
+    return TM_OK;
+}
+
 int tm_set_memory_budget(tm_engine *e, uint64_t bytes) {
     if (!e || bytes == 0) return TM_ERR_INVALID;
     e->eng.set_memory_budget(bytes);

@@ -574,6 +574,12 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
     uint32_t nq = 0;
     for (const Piece &p : pieces) nq += p.n;
     bool ok = true;
+    // results left on the device: only for whole requests with a request
+    // callback (per-query handlers and split requests get host copies)
+    bool dres = device_results_.load();
+    for (const Piece &p : pieces)
+        if (p.r->qcb || p.q0 != 0 || p.n != p.r->n) dres = false;
+    const uint32_t *dkeys_out = nullptr;
     try {
         ln.h_queries.reserve(size_t(nq) * kWords);
         uint32_t at = 0;
@@ -596,8 +602,9 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
         ln.h_offsets.reserve(size_t(nq) + 1);
         ln.h_keys.reserve(std::max<uint64_t>(nk, 1));
         TM_CUDA(cudaMemcpyAsync(ln.h_offsets.p, doff, (size_t(nq) + 1) * 8, cudaMemcpyDeviceToHost, ln.stream));
-        if (nk) TM_CUDA(cudaMemcpyAsync(ln.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, ln.stream));
+        if (nk && !dres) TM_CUDA(cudaMemcpyAsync(ln.h_keys.p, dkeys, nk * 4, cudaMemcpyDeviceToHost, ln.stream));
         TM_CUDA(cudaStreamSynchronize(ln.stream));
+        dkeys_out = dkeys;
         // running estimate of device bytes per query (queues, hit records, keys)
         const uint64_t bytes = bs.routed * (kQueueWords * 4) + bs.records * sizeof(HitRec) + nk * 4 * (unique ? 3 : 1);
         const uint64_t bpq = std::max<uint64_t>(1024, bytes / std::max<uint32_t>(nq, 1));
@@ -608,7 +615,7 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
         async_error_ = e.what();
     }
     const uint64_t *off = ln.h_offsets.p;
-    const uint32_t *keys = ln.h_keys.p;
+    const uint32_t *keys = dres ? dkeys_out : ln.h_keys.p;
     uint32_t at = 0;
     std::vector<uint64_t> rebased;
     for (Piece &p : pieces) {

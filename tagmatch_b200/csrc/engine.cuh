@@ -182,6 +182,9 @@ public:
     TrainReport train_scheduler(uint32_t epochs);
     void set_learned_order(bool on) { learned_order_.store(on); }
     void set_latency_target_ms(uint32_t ms) { latency_target_ms_.store(ms ? ms : 1); }
+    // serving results left in device memory (request callbacks get a device
+    // pointer to their keys) instead of copied to the host
+    void set_device_results(bool on) { device_results_.store(on); }
     bool started() const { return started_; }
     // host copy of the consolidated filters (table order) and keys
     const std::vector<uint32_t> &filters() const { return filters_; }
@@ -281,6 +284,7 @@ private:
     Scheduler sched_;
     std::atomic<bool> learned_order_{false};
     std::atomic<uint32_t> latency_target_ms_{25};
+    std::atomic<bool> device_results_{false};
     // arrival rate of asynchronous queries (queue lock)
     uint64_t arrived_queries_ = 0, rate_q_ = 0;
     std::chrono::steady_clock::time_point rate_t_{};

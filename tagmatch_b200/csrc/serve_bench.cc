@@ -19,8 +19,11 @@
 // usage: tagmatch_serve_bench [filters=N] [pool=Q] [seed=S] [maxp=P]
 //          [rates=r1,r2,...] [modes=plain,continuous,learned] [seconds=T]
 //          [unique=0|1] [target_ms=M] [calib=T] [epochs=E] [plain_rates=...]
+//          [results=host,device]
 // (plain_rates: the rates of the plain mode, which saturates far below the
-// others; default: rates)
+// others; default: rates.  results: where the keys go, each in turn --
+// host memory, or left in device memory (TM_RESULTS_DEVICE); every line
+// says which.)
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -80,7 +83,8 @@ double pct(std::vector<double> &v, double p) {
 int main(int argc, char **argv) {
     uint64_t filters = 10000000, pool = 1 << 20, seed = 2;
     uint32_t maxp = 65536;
-    std::string rates = "100000,300000,1000000", modes = "plain,continuous", plain_rates;
+    std::string rates = "100000,300000,1000000", modes = "plain,continuous", plain_rates, results = "host";
+    std::string residency = "host";
     double seconds = 5.0, calib = 3.0;
     int unique = 0;
     uint32_t target_ms = 25, epochs = 30;
@@ -93,6 +97,7 @@ int main(int argc, char **argv) {
         else if (a.rfind("maxp=", 0) == 0) maxp = uint32_t(std::stoul(v));
         else if (a.rfind("rates=", 0) == 0) rates = v;
         else if (a.rfind("plain_rates=", 0) == 0) plain_rates = v;
+        else if (a.rfind("results=", 0) == 0) results = v;
         else if (a.rfind("modes=", 0) == 0) modes = v;
         else if (a.rfind("seconds=", 0) == 0) seconds = std::stod(v);
         else if (a.rfind("unique=", 0) == 0) unique = std::stoi(v);
@@ -172,39 +177,43 @@ int main(int argc, char **argv) {
         }
         const double span = std::chrono::duration<double>(last - t0).count();
         std::printf(
-            "{\"mode\": \"%s\", \"offered_qps\": %.0f, \"sustained_qps\": %.0f, \"requests\": %zu, \"queries\": %llu, "
-            "\"p50_ms\": %.3f, \"p99_ms\": %.3f, \"p999_ms\": %.3f, \"keys\": %llu, \"unique\": %d}\n",
-            label, rate, queries / std::max(span, 1e-9), t_arr.size(), (unsigned long long)queries, pct(lat, 0.50),
-            pct(lat, 0.99), pct(lat, 0.999), (unsigned long long)g_keys.load(), unique);
+            "{\"mode\": \"%s\", \"results\": \"%s\", \"offered_qps\": %.0f, \"sustained_qps\": %.0f, \"requests\": %zu, "
+            "\"queries\": %llu, \"p50_ms\": %.3f, \"p99_ms\": %.3f, \"p999_ms\": %.3f, \"keys\": %llu, \"unique\": %d}\n",
+            label, residency.c_str(), rate, queries / std::max(span, 1e-9), t_arr.size(), (unsigned long long)queries,
+            pct(lat, 0.50), pct(lat, 0.99), pct(lat, 0.999), (unsigned long long)g_keys.load(), unique);
         std::fflush(stdout);
         return true;
     };
-    bool trained = false;
-    for (const std::string &mode : split(modes)) {
-        int fm = mode == "plain" ? TM_FLUSH_SINGLE : mode == "learned" ? TM_FLUSH_LEARNED : TM_FLUSH_IMMEDIATE;
-        if (mode == "learned" && !trained) {
-            // calibration: timing samples from continuous serving, then training
-            tm_sched_record(e, 1);
-            if (!run(TM_FLUSH_IMMEDIATE, std::stod(split(rates).front()), calib, "calibration", false)) return 2;
-            tm_sched_record(e, 0);
-            tm_sched_report rep{};
-            if (tm_sched_train(e, epochs, &rep) != TM_OK) {
-                std::fprintf(stderr, "training failed: %s\n", tm_last_error(e));
-                return 2;
+    for (const std::string &res : split(results)) {
+        residency = res;
+        tm_set_serving_results(e, res == "device" ? TM_RESULTS_DEVICE : TM_RESULTS_HOST);
+        bool trained = false;
+        for (const std::string &mode : split(modes)) {
+            int fm = mode == "plain" ? TM_FLUSH_SINGLE : mode == "learned" ? TM_FLUSH_LEARNED : TM_FLUSH_IMMEDIATE;
+            if (mode == "learned" && !trained) {
+                // calibration: timing samples from continuous serving, then training
+                tm_sched_record(e, 1);
+                if (!run(TM_FLUSH_IMMEDIATE, std::stod(split(rates).front()), calib, "calibration", false)) return 2;
+                tm_sched_record(e, 0);
+                tm_sched_report rep{};
+                if (tm_sched_train(e, epochs, &rep) != TM_OK) {
+                    std::fprintf(stderr, "training failed: %s\n", tm_last_error(e));
+                    return 2;
+                }
+                double p1k = 0, p16k = 0;
+                tm_sched_predict_batch_ms(e, 1024, &p1k);
+                tm_sched_predict_batch_ms(e, 16384, &p16k);
+                std::printf("{\"mode\": \"learned-training\", \"results\": \"%s\", \"samples\": %llu, \"steps\": %llu, "
+                            "\"train_mse\": %.4f, \"val_mse\": %.4f, \"val_r2\": %.4f, \"mean_mse\": %.4f, "
+                            "\"train_ms\": %.1f, \"pred_ms_1024\": %.3f, \"pred_ms_16384\": %.3f, \"target_ms\": %u}\n",
+                            residency.c_str(), (unsigned long long)rep.samples, (unsigned long long)rep.steps,
+                            rep.train_mse, rep.val_mse, rep.val_r2, rep.mean_mse, rep.ms, p1k, p16k, target_ms);
+                std::fflush(stdout);
+                trained = true;
             }
-            double p1k = 0, p16k = 0;
-            tm_sched_predict_batch_ms(e, 1024, &p1k);
-            tm_sched_predict_batch_ms(e, 16384, &p16k);
-            std::printf("{\"mode\": \"learned-training\", \"samples\": %llu, \"steps\": %llu, \"train_mse\": %.4f, "
-                        "\"val_mse\": %.4f, \"val_r2\": %.4f, \"mean_mse\": %.4f, \"train_ms\": %.1f, "
-                        "\"pred_ms_1024\": %.3f, \"pred_ms_16384\": %.3f, \"target_ms\": %u}\n",
-                        (unsigned long long)rep.samples, (unsigned long long)rep.steps, rep.train_mse, rep.val_mse,
-                        rep.val_r2, rep.mean_mse, rep.ms, p1k, p16k, target_ms);
-            std::fflush(stdout);
-            trained = true;
+            for (const std::string &rs : split(mode == "plain" && !plain_rates.empty() ? plain_rates : rates))
+                if (!run(fm, std::stod(rs), seconds, mode.c_str(), true)) return 2;
         }
-        for (const std::string &rs : split(mode == "plain" && !plain_rates.empty() ? plain_rates : rates))
-            if (!run(fm, std::stod(rs), seconds, mode.c_str(), true)) return 2;
     }
     tm_destroy(e);
     return 0;

@@ -212,10 +212,21 @@ class TagMatch:
     def set_memory_budget(self, nbytes):
         self._check(self._lib.tm_set_memory_budget(self._h, nbytes))
 
+    def set_serving_results(self, where):
+        """TM_RESULTS_HOST or TM_RESULTS_DEVICE (request keys left in device
+        memory; this wrapper copies them out inside the callback)."""
+        self._check(self._lib.tm_set_serving_results(self._h, where))
+        self._device_results = where == _native.TM_RESULTS_DEVICE
+
     def _on_request(self, user, tag, offsets, keys, n, status):
         off = np.ctypeslib.as_array(offsets, shape=(n + 1,)).copy()
         nk = int(off[-1])
-        arr = np.ctypeslib.as_array(keys, shape=(nk,)).copy() if nk else np.zeros(0, dtype=np.uint32)
+        if not nk:
+            arr = np.zeros(0, dtype=np.uint32)
+        elif getattr(self, "_device_results", False):
+            arr = read_device(ctypes.cast(keys, ctypes.c_void_p).value, nk, np.uint32)
+        else:
+            arr = np.ctypeslib.as_array(keys, shape=(nk,)).copy()
         with self._cb_lock:
             h = self._callbacks.pop(tag, None)
         if h is not None:

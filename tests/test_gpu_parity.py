@@ -306,11 +306,13 @@ def test_config1_large_work_items_device_batch(seg_tiles):
     tm.close()
 
 
+@pytest.mark.parametrize("results", [_native.TM_RESULTS_HOST, _native.TM_RESULTS_DEVICE])
 @pytest.mark.parametrize("mode", [_native.TM_FLUSH_IMMEDIATE, _native.TM_FLUSH_SINGLE, _native.TM_FLUSH_FULL_OR_LATENCY])
-def test_submit_requests_same_alone_and_mixed(mode):
+def test_submit_requests_same_alone_and_mixed(mode, results):
     """Serving: requests of 1..700 queries, merged into shared device batches
     (or one per batch), split across batches when the batch limit is small;
-    each request's result equals the same queries matched alone."""
+    each request's result equals the same queries matched alone, with the
+    keys returned in host memory or left in device memory."""
     f, ko, k = workload.generate_filters(30000, 44)
     q = workload.generate_queries(3000, f, 44)
     tm = engine_with(f, ko, k, 4096)
@@ -334,6 +336,7 @@ def test_submit_requests_same_alone_and_mixed(mode):
         return h
 
     tm.set_flush_mode(mode)
+    tm.set_serving_results(results)
     tm.set_batch_limit(1000)  # forces merging and splitting
     tm.set_latency_limit_ms(2)
     tm.start(4, 1)
