@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-rates", default="250000,500000,750000,1000000,1500000")
-    ap.add_argument("--serve-plain-rates", default="100000,150000,200000,300000")
+    ap.add_argument("--serve-plain-rates", default="100000,200000,300000,450000,600000")
     ap.add_argument("--serve-modes", default="plain,continuous,learned")
     ap.add_argument("--serve-results", default="host,device")
     ap.add_argument("--latency-target-ms", type=int, default=25)
