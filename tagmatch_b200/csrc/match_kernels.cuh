@@ -616,19 +616,28 @@ inline void launch_match(const MatchArgs &a, unsigned grid, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Key gather
 // ---------------------------------------------------------------------------
-constexpr int kFillPerLane = 4;  // records per lane per warp step (loads in flight)
+// records per lane per warp step (loads in flight) and the gather's
+// minimum resident CTAs per SM (register budget); build-time tunables
+#ifndef TM_FILL_PER_LANE
+#define TM_FILL_PER_LANE 2
+#endif
+#ifndef TM_FILL_MIN_CTAS
+#define TM_FILL_MIN_CTAS 6
+#endif
+constexpr int kFillPerLane = TM_FILL_PER_LANE;
 
 // Copies every record's keys into its query's range (qoff).  Each record's
 // keys are reserved with one atomic on the query's cursor (qcursor, zeroed
-// by the caller).  A warp takes 4 x 32 records per step, so that the four
+// by the caller).  A warp takes 2 x 32 records per step, so that the four
 // dependent load levels (record -> cursor and key start -> keys) each have
-// four requests in flight per lane.  Records whose hits form one run of
-// adjacent bits (the usual case) have one contiguous key range; the warp
-// copies the ranges of 32 such records together, 32 keys per step: a prefix
-// sum over the lanes' key counts, and for key j of the warp a 5-step shuffle
-// search for the lane that owns it.  Records with several runs copy their
-// own ranges.
-__global__ void __launch_bounds__(256) k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
+// two requests in flight per lane (6 CTAs per SM).  A run of adjacent hit bits is one
+// contiguous key range of the tile's slots; the warp copies one run per
+// lane per round together, 32 keys per step: a prefix sum over the lanes'
+// run lengths, and for key j of the round a 5-step shuffle search for the
+// lane that owns it.  Single-run records (the usual case) take one round;
+// the further runs of the others take further rounds, so no lane copies
+// keys on its own.
+__global__ void __launch_bounds__(256, TM_FILL_MIN_CTAS) k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
                                                   const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
                                                   const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor,
                                                   uint32_t *__restrict__ out) {
@@ -662,42 +671,52 @@ __global__ void __launch_bounds__(256) k_key_fill(const HitRec *__restrict__ rec
         }
 #pragma unroll
         for (int j = 0; j < kFillPerLane; ++j) {
-            // several runs: this lane copies its own ranges
-            if (nk[j] && !single[j]) {
-                const uint32_t *o = slot_key_off + size_t(r[j].tile) * kTile;
-                uint64_t d = dst[j];
-                uint64_t m = r[j].mask;
-                while (m) {  // runs of adjacent hit bits, as in for_each_key_run
+            // the warp copies one run of adjacent hit bits per lane per round
+            // (a single-run record in one round; the runs of other records
+            // in further rounds), 32 keys per step
+            const uint32_t *o = slot_key_off + size_t(r[j].tile) * kTile;
+            uint64_t m = nk[j] ? r[j].mask : 0u;
+            uint64_t d = dst[j];
+            bool first = true;
+            while (__any_sync(kFull, m != 0)) {
+                uint32_t len = 0, s = 0;
+                if (m) {
                     const int lo = __ffsll(m) - 1;
-                    const uint64_t filled = m + (1ull << lo);
+                    const uint64_t filled = m + (1ull << lo);  // the carry clears the run and sets bit hi
                     const int hi = __ffsll(filled & ~m) - 1;
-                    for (uint32_t k = o[lo], e = o[hi]; k < e; ++k) out[d++] = tkeys[k];
+                    if (first && single[j]) {
+                        s = src[j];
+                        len = nk[j];
+                    } else {
+                        s = o[lo];
+                        len = o[hi] - s;
+                    }
                     m &= filled;
                 }
-            }
-            // one run: the warp copies all such ranges together
-            const uint32_t cnk = single[j] ? nk[j] : 0u;
-            uint32_t incl = cnk;
+                first = false;
+                uint32_t incl = len;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t v = __shfl_up_sync(kFull, incl, d);
-                if (lane >= (unsigned)d) incl += v;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            const uint32_t start = incl - cnk;  // this lane's first key among the warp's
-            for (uint32_t j0 = 0; j0 < total; j0 += 32) {
-                const uint32_t k = j0 + lane;
-                // owner: the first lane whose inclusive count exceeds k
-                uint32_t owner = 0;
-#pragma unroll
-                for (int step = 16; step >= 1; step >>= 1) {
-                    const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
-                    if (v <= k) owner += step;
+                for (int step = 1; step < 32; step <<= 1) {
+                    const uint32_t v = __shfl_up_sync(kFull, incl, step);
+                    if (lane >= (unsigned)step) incl += v;
                 }
-                const uint32_t ostart = __shfl_sync(kFull, start, owner);
-                const uint32_t osrc = __shfl_sync(kFull, src[j], owner);
-                const uint64_t odst = __shfl_sync(kFull, dst[j], owner);
-                if (k < total) out[odst + (k - ostart)] = tkeys[osrc + (k - ostart)];
+                const uint32_t total = __shfl_sync(kFull, incl, 31);
+                const uint32_t start = incl - len;  // this lane's first key among the round's
+                for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+                    const uint32_t k = j0 + lane;
+                    // owner: the first lane whose inclusive count exceeds k
+                    uint32_t owner = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
+                        if (v <= k) owner += step;
+                    }
+                    const uint32_t ostart = __shfl_sync(kFull, start, owner);
+                    const uint32_t osrc = __shfl_sync(kFull, s, owner);
+                    const uint64_t odst = __shfl_sync(kFull, d, owner);
+                    if (k < total) out[odst + (k - ostart)] = tkeys[osrc + (k - ostart)];
+                }
+                d += len;
             }
         }
     }
