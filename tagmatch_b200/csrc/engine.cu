@@ -50,6 +50,8 @@ Engine::~Engine() {
             if (h.staged) cudaEventDestroy(h.staged);
             for (cudaEvent_t ev : h.trace_ev)
                 if (ev) cudaEventDestroy(ev);
+            for (cudaEvent_t ev : h.copy_ev)
+                if (ev) cudaEventDestroy(ev);
         }
     }
 }
@@ -883,10 +885,20 @@ double host_batch_keys() {
     return s && *s ? std::max(0.0, std::atof(s)) : kHostBatchKeys;
 }
 
-double direct_fraction() {
+// TM_DIRECT_FRACTION fixes the direct share; otherwise (< 0) it adapts.
+double direct_fraction_fixed() {
     const char *s = std::getenv("TM_DIRECT_FRACTION");
-    if (!s || !*s) return kDirectFraction;
+    if (!s || !*s) return -1.0;
     return std::min(1.0, std::max(0.0, std::atof(s)));
+}
+
+// The direct share that balances the two host-side stages of a batch: the
+// link carries 2 bytes per narrowed key and 4 per direct key at c bytes/ms,
+// host threads widen the narrowed keys at w keys/ms; both take the same
+// time when (1 - f) / w = (2 (1 - f) + 4 f) / c, i.e. f = (c - 2w) / (c + 2w).
+double balanced_direct_fraction(double c, double w) {
+    const double f = (c - 2.0 * w) / (c + 2.0 * w);
+    return std::min(0.75, std::max(0.0, f));
 }
 
 }  // namespace
@@ -895,10 +907,13 @@ double direct_fraction() {
 // one batch is matched, the results of the two before it cross PCIe and are
 // widened, so the device never waits for the host copies of the batch it
 // last finished.  Keys go to the caller's buffer in one of three ways:
-// - every key of the table below 65,536: a share direct_fraction() of the
-//   batch's keys is copied as 32-bit values straight into a pinned caller
-//   buffer; the rest crosses as 16-bit values into pinned staging and copy
-//   threads widen them into the caller's buffer;
+// - every key of the table below 65,536: a share of the batch's keys is
+//   copied as 32-bit values straight into a pinned caller buffer; the rest
+//   crosses as 16-bit values into pinned staging and copy threads widen
+//   them into the caller's buffer.  The share adapts from batch to batch:
+//   each large batch's measured link rate (CUDA events around its copies)
+//   and widening rate give the share that balances the two, and the
+//   engine moves halfway to it (TM_DIRECT_FRACTION fixes it instead);
 // - otherwise, pinned caller buffer: one 32-bit copy straight into it;
 // - otherwise: a 32-bit copy into pinned staging, then copy threads.
 void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint64_t *out_offsets, uint32_t *out_keys,
@@ -929,7 +944,12 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
     }
     const bool narrow = d.table.max_key < 65536u;
     const bool pinned_out = out_keys != nullptr && is_pinned(out_keys);
-    const double frac = pinned_out ? direct_fraction() : 0.0;
+    const double fixed_frac = direct_fraction_fixed();
+    const bool adapt = pinned_out && narrow && fixed_frac < 0;
+    if (direct_frac_ < 0) direct_frac_ = kDirectFraction;
+    for (int l = 0; l < kHostLanes && adapt; ++l)
+        for (cudaEvent_t &ev : d.host[l].copy_ev)
+            if (!ev) TM_CUDA(cudaEventCreate(&ev));
     const double batch_keys = host_batch_keys();
     struct Pending {
         bool active = false;
@@ -954,10 +974,21 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             cudaEventElapsedTime(&m32, d.host[l].trace_ev[1], d.host[l].trace_ev[2]);
             std::fprintf(stderr,
                          "[tm host] batch %llu lane %d keys %llu direct %llu begin %.1f matched %.1f widen %.1f-%.1f "
-                         "narrow_copy_ms %.1f direct_copy_ms %.1f finish_wait_ms %.1f\n",
+                         "narrow_copy_ms %.1f direct_copy_ms %.1f finish_wait_ms %.1f direct_share %.3f\n",
                          (unsigned long long)p.batch, l, (unsigned long long)p.nk, (unsigned long long)p.nd,
                          ms_at(p.t_begin), ms_at(p.t_matched), ms_at(p.t_widen0), ms_at(p.t_widen1), m16, m32,
-                         ms_at(TClock::now()) - ms_at(t_wait));
+                         ms_at(TClock::now()) - ms_at(t_wait), direct_frac_);
+        }
+        if (adapt && p.nk - p.nd >= (uint64_t(1) << 26)) {
+            // link and widening rates of this batch -> the balancing share
+            float copy_ms = 0.f;
+            const double widen_ms = std::chrono::duration<double, std::milli>(p.t_widen1 - p.t_widen0).count();
+            if (cudaEventElapsedTime(&copy_ms, d.host[l].copy_ev[0], d.host[l].copy_ev[1]) == cudaSuccess &&
+                copy_ms > 0.f && widen_ms > 0.0) {
+                const double c = double(2 * (p.nk - p.nd) + 4 * p.nd) / copy_ms;
+                const double w = double(p.nk - p.nd) / widen_ms;
+                direct_frac_ = 0.5 * direct_frac_ + 0.5 * balanced_direct_fraction(c, w);
+            }
         }
         const uint64_t *o = d.host[l].h_offsets.p;
         for (uint32_t i = 1; i <= p.n; ++i) out_offsets[p.q0 + i] = o[i] + p.base;
@@ -1017,11 +1048,13 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
                 if (narrow) {
                     // keys [0, nd) direct, [nd, nk) narrowed; nd a multiple
                     // of 4 keeps the narrowing kernel on 16-byte loads
+                    const double frac = !pinned_out ? 0.0 : fixed_frac >= 0 ? fixed_frac : direct_frac_;
                     const uint64_t nd = std::min<uint64_t>(nk, uint64_t(double(nk) * frac) & ~uint64_t(3));
                     const uint64_t nn = nk - nd;
                     p.nd = nd;
                     if (nn) {
                         const uint16_t *d16 = narrow_keys(dkeys + nd, nn, sc, str[l]);
+                        if (adapt) TM_CUDA(cudaEventRecord(h.copy_ev[0], str[l]));
                         h.h_keys16.reserve(nn);
                         TM_CUDA(cudaMemcpyAsync(h.h_keys16.p, d16, nn * 2, cudaMemcpyDeviceToHost, str[l]));
                         TM_CUDA(cudaEventRecord(h.staged, str[l]));
@@ -1031,13 +1064,16 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
                         Pending *pp = &p;
                         p.copier = std::thread([=] {
                             if (cudaEventSynchronize(ev) != cudaSuccess) return;
-                            if (trace) pp->t_widen0 = TClock::now();
+                            pp->t_widen0 = TClock::now();
                             parallel_widen(wdst, src, nn);
-                            if (trace) pp->t_widen1 = TClock::now();
+                            pp->t_widen1 = TClock::now();
                         });
+                    } else if (adapt) {
+                        TM_CUDA(cudaEventRecord(h.copy_ev[0], str[l]));
                     }
                     if (trace) TM_CUDA(cudaEventRecord(h.trace_ev[1], str[l]));
                     if (nd) TM_CUDA(cudaMemcpyAsync(dst, dkeys, nd * 4, cudaMemcpyDeviceToHost, str[l]));
+                    if (adapt) TM_CUDA(cudaEventRecord(h.copy_ev[1], str[l]));
                     if (trace) TM_CUDA(cudaEventRecord(h.trace_ev[2], str[l]));
                     stats_.d2h_bytes += nn * 2 + nd * 4;
                 } else if (pinned_out) {

@@ -214,6 +214,7 @@ private:
         cudaStream_t stream = nullptr;
         cudaEvent_t staged = nullptr;
         cudaEvent_t trace_ev[3] = {nullptr, nullptr, nullptr};  // TM_HOST_TRACE: matched, narrow copied, direct copied
+        cudaEvent_t copy_ev[2] = {nullptr, nullptr};            // around a batch's key copies (direct share)
         HostBuf<uint64_t> h_offsets;
         HostBuf<uint32_t> h_keys;
         HostBuf<uint16_t> h_keys16;
@@ -267,6 +268,7 @@ private:
     int base_device_ = 0;
     uint32_t seg_tiles_ = kSegTiles;
     double host_keys_per_query_ = 0;  // output keys per query of match_host's last batch
+    double direct_frac_ = -1;         // match_host's adaptive direct share (< 0: not yet set)
 
     // async path
     std::mutex q_mtx_;

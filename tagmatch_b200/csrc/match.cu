@@ -265,8 +265,8 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
             TM_CUDA(cudaMemcpy(w, s.work.p, sizeof(w), cudaMemcpyDeviceToHost));
             std::fprintf(stderr,
                          "[tm work] queries %u tile_visits %llu query_passes %llu candidates %llu filter_trips %llu "
-                         "items %llu query_groups %llu records %llu pairs %llu\n",
-                         nq, w[0], w[1], w[2], w[3], w[4], w[5], hc[1], hc[3]);
+                         "items %llu query_groups %llu query_lanes %llu small_query_visits %llu records %llu pairs %llu\n",
+                         nq, w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7], hc[1], hc[3]);
         }
         if (s.profile) {
             float ms = 0.f;

@@ -211,7 +211,8 @@ struct MatchArgs {
     // optional work counters (diagnostics): [0] tile visits, [1] passes of
     // the lane-per-query path, [2] candidate (query, tile) pairs, [3] trips
     // of the lane-per-filter path, [4] items, [5] 4-filter groups tested by
-    // the lane-per-query path; null when off
+    // the lane-per-query path, [6] its busy lanes summed over passes, [7]
+    // its tile visits with at most 16 candidates; null when off
     unsigned long long *work;
 };
 
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
         S.inflight = produce(a, total, S, 0) ? 1u : 0u;
         S.inflight_par = 0;
     }
-    uint32_t w_tiles = 0, w_passes = 0, w_cand = 0, w_trips = 0, w_items = 0, w_groups = 0;
+    uint32_t w_tiles = 0, w_passes = 0, w_cand = 0, w_trips = 0, w_items = 0, w_groups = 0, w_lanes = 0, w_small = 0;
     uint32_t wn = 0;      // records staged by this warp (warp-uniform)
     uint32_t w_recs = 0;  // records this warp has produced (warp-uniform)
     uint32_t pairs = 0;  // matching (query, filter) pairs found by this lane
@@ -452,6 +453,8 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                         if (COUNT) {
                             ++w_passes;
                             w_groups += groups;
+                            w_lanes += min(32u, n - p0);
+                            if (p0 == 0 && n <= 16) ++w_small;
                         }
                         const uint32_t j = p0 + lane;
                         const uint32_t c2 = j < n ? 2u * lst[j] : 0u;
@@ -585,6 +588,8 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
         atomicAdd(&a.work[2], (unsigned long long)w_cand);
         atomicAdd(&a.work[3], (unsigned long long)w_trips);
         atomicAdd(&a.work[5], (unsigned long long)w_groups);
+        atomicAdd(&a.work[6], (unsigned long long)w_lanes);
+        atomicAdd(&a.work[7], (unsigned long long)w_small);
         if (warp == 0) atomicAdd(&a.work[4], (unsigned long long)w_items);
     }
     // no copy may still target this CTA's shared memory when it exits: after
