@@ -168,10 +168,13 @@ int tm_submit(tm_engine *e, const uint32_t *queries, uint32_t n, int unique, uin
  * TM_FLUSH_LEARNED: continuous batching whose flush points come from the
  *   learned cost model (tm_sched_train): a free lane takes the pending
  *   requests once they make a batch that keeps up with the measured
- *   arrival rate (queries over the batch's predicted time >= 1.25 x the
- *   rate), or once the oldest one's wait plus the batch's predicted time
- *   reaches half the latency target (tm_set_latency_target_ms); before
- *   training it behaves as TM_FLUSH_IMMEDIATE. */
+ *   arrival rate (the two lanes' queries over the batch's predicted time
+ *   >= 1.25 x the rate), or once the oldest one's wait plus the batch's predicted time
+ *   reaches half the latency target (tm_set_latency_target_ms); each batch
+ *   also runs at the tiles per work item with the lowest predicted time
+ *   (32 .. 8,192), so the model should be trained on samples recorded at
+ *   several of those values; before training it behaves as
+ *   TM_FLUSH_IMMEDIATE. */
 #define TM_FLUSH_FULL_OR_LATENCY 0
 #define TM_FLUSH_IMMEDIATE 1
 #define TM_FLUSH_SINGLE 2

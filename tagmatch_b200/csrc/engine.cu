@@ -521,7 +521,7 @@ void Engine::worker_loop(int dev, int lane) {
                         const auto now = std::chrono::steady_clock::now();
                         const double age = std::chrono::duration<double, std::milli>(now - pending_.front()->arrived).count();
                         const double budget = 0.5 * latency_target_ms_.load();
-                        const uint32_t need = sched_.stable_batch(arrival_qps_, cap);
+                        const uint32_t need = sched_.stable_batch(arrival_qps_, cap, kLanes);
                         if (b0 >= need || age + t0 >= budget) break;
                         double wait_ms = budget - age - t0;
                         if (arrival_qps_ > 0) wait_ms = std::min(wait_ms, 1e3 * double(need - b0) / arrival_qps_);
@@ -596,7 +596,7 @@ void Engine::run_pieces(Device &d, Lane &ln, std::vector<Piece> &pieces, bool un
         const uint32_t *dkeys;
         uint64_t nk = 0;
         BatchStats bs;
-        prepare(ln.scratch);
+        prepare(ln.scratch, nq, true);
         const auto tb = std::chrono::steady_clock::now();
         match_batch(d.table, ln.scratch.queries.p, nq, unique, ln.scratch, &doff, &dkeys, &nk, &bs, ln.stream);
         observe(d.table, ln.scratch, nq, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count(),
@@ -671,7 +671,7 @@ void Engine::match_device(const uint32_t *d_queries, uint32_t nq, bool unique, c
     TM_CUDA(cudaSetDevice(d.id));
     BatchStats local;
     d.scratch.profile = profile_;
-    prepare(d.scratch);
+    prepare(d.scratch, nq, false);
     const auto tb = std::chrono::steady_clock::now();
     match_batch(d.table, d_queries, nq, unique, d.scratch, d_offsets, d_keys, n_keys, &local, st ? st : d.stream, ev0, ev1);
     observe(d.table, d.scratch, nq, std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count(),
@@ -753,14 +753,22 @@ void Engine::autotune(const uint32_t *queries, uint32_t n, uint32_t *seg_out, ui
     *qps_out = best;
 }
 
-void Engine::prepare(MatchScratch &s) {
+void Engine::prepare(MatchScratch &s, uint32_t nq, bool serving) {
     s.record_items = sched_.recording();
     if (learned_order_.load()) s.part_order = sched_.order();
     else s.part_order.clear();
+    if (serving) {
+        // the learned serving mode also picks each batch's tiles per work
+        // item (small batches want more, smaller items); otherwise the
+        // engine's (autotuned) value
+        const uint32_t best = flush_mode_.load() == kFlushLearned ? sched_.best_seg(nq) : 0u;
+        s.seg_tiles = best ? best : seg_tiles_;
+    }
 }
 
 void Engine::observe(const DevTable &t, const MatchScratch &s, uint32_t nq, double ms, uint64_t keys) {
     if (s.record_items) sched_.absorb(t, s, nq, ms, keys);
+    else if (flush_mode_.load() == kFlushLearned) sched_.observe_batch(nq, ms);
 }
 
 TrainReport Engine::train_scheduler(uint32_t epochs) {
@@ -1022,7 +1030,7 @@ void Engine::match_host(const uint32_t *queries, uint64_t nq, bool unique, uint6
             uint64_t nk = 0;
             BatchStats bs;
             sc.profile = profile_;
-            prepare(sc);
+            prepare(sc, n, false);
             match_batch(d.table, sc.queries.p, n, unique, sc, &doff, &dkeys, &nk, &bs, str[l]);
             observe(d.table, sc, n, std::chrono::duration<double, std::milli>(TClock::now() - t_begin).count(), nk);
             stats_.add(bs, n, profile_);

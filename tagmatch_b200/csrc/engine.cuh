@@ -232,7 +232,7 @@ private:
     };
     void build_device_table(Device &d);
     // before / after every batch: work-queue order and timing record
-    void prepare(MatchScratch &s);
+    void prepare(MatchScratch &s, uint32_t nq, bool serving);
     void observe(const DevTable &t, const MatchScratch &s, uint32_t nq, double ms, uint64_t keys);
     void apply_seg_tiles(uint32_t seg);
     void consolidate_bulk();

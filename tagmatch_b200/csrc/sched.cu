@@ -402,6 +402,9 @@ void item_features(float *x, uint32_t part_size, uint32_t mask_bits, uint32_t qu
 namespace {
 constexpr size_t kMaxSamples = size_t(4) << 20;
 constexpr int kTableSteps = 19;  // b = 1 .. 2^18
+// candidate tiles per work item (the autotuner's range)
+constexpr int kSegChoices = 9;
+constexpr uint32_t kSegChoice[kSegChoices] = {32, 64, 128, 256, 512, 1024, 2048, 4096, 8192};
 
 uint32_t mask_bits(const DevTable &t, uint32_t p) {
     uint32_t c = 0;
@@ -482,7 +485,7 @@ void Scheduler::absorb(const DevTable &t, const MatchScratch &s, uint32_t nq, do
     }
     const double kpq = double(keys) / nq;
     keys_per_query_ = obs_.empty() ? kpq : 0.8 * keys_per_query_ + 0.2 * kpq;
-    if (obs_.size() < 4096) obs_.push_back({double(nq), batch_ms, double(keys)});
+    if (obs_.size() < 4096) obs_.push_back({double(nq), batch_ms, double(keys), double(seg)});
 }
 
 TrainReport Scheduler::train(const DevTable &t, uint32_t seg_tiles, int sm_count, double clock_hz, uint32_t epochs,
@@ -494,30 +497,34 @@ TrainReport Scheduler::train(const DevTable &t, uint32_t seg_tiles, int sm_count
 }
 
 // Predicted warp-cycles of every partition's items for batches of 2^k
-// queries (routed in the recent fractions), turned into kernel time over
-// the device's matcher CTAs; then a least-squares fit of the measured batch
-// times on (1, predicted kernel ms, keys).  Also the work-queue order.
+// queries (routed in the recent fractions), for every candidate number of
+// tiles per work item, turned into kernel time over the device's matcher
+// CTAs: the larger of the summed item time spread over the CTAs and the
+// longest item (one CTA runs an item; its 8 warps' cycles add up).  Then a
+// least-squares fit of the measured batch times on (1, predicted kernel
+// ms, keys).  Also the work-queue order.
 void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, double clock_hz, cudaStream_t st) {
     const uint32_t P = t.n_parts;
     if (P == 0 || frac_.size() != P || !model_.trained()) return;
-    // rows: [k][p][full chunk, partial chunk], then the order rows [p]
-    const size_t rows = size_t(kTableSteps) * P * 2 + P;
+    // rows: [s][k][p][full chunk, partial chunk], then the order rows [p]
+    const size_t per_seg = size_t(kTableSteps) * P * 2;
+    const size_t rows = size_t(kSegChoices) * per_seg + P;
     std::vector<float> x(rows * kMlpIn), y(rows);
-    std::vector<uint32_t> nfull(size_t(kTableSteps) * P), rem(size_t(kTableSteps) * P);
-    for (int k = 0; k < kTableSteps; ++k) {
-        const double b = double(1u << k);
-        for (uint32_t p = 0; p < P; ++p) {
-            const uint32_t tiles = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
-            const uint32_t ns = std::max<uint32_t>(1, (tiles + seg - 1) / seg);
-            const uint32_t ts = (tiles + ns - 1) / ns;
-            const uint32_t cnt = uint32_t(std::llround(b * frac_[p]));
-            nfull[size_t(k) * P + p] = cnt / kChunk;
-            rem[size_t(k) * P + p] = cnt % kChunk;
-            const float dens = std::max(density_[p], 0.f);
-            const size_t r0 = (size_t(k) * P + p) * 2;
-            item_features(&x[r0 * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt, kChunk, ts, dens, tiles, seg);
-            item_features(&x[(r0 + 1) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt, std::max<uint32_t>(1, cnt % kChunk),
-                          ts, dens, tiles, seg);
+    for (int si = 0; si < kSegChoices; ++si) {
+        const uint32_t sg = kSegChoice[si];
+        for (int k = 0; k < kTableSteps; ++k) {
+            const double b = double(1u << k);
+            for (uint32_t p = 0; p < P; ++p) {
+                const uint32_t tiles = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
+                const uint32_t ns = std::max<uint32_t>(1, (tiles + sg - 1) / sg);
+                const uint32_t ts = (tiles + ns - 1) / ns;
+                const uint32_t cnt = uint32_t(std::llround(b * frac_[p]));
+                const float dens = std::max(density_[p], 0.f);
+                const size_t r0 = size_t(si) * per_seg + (size_t(k) * P + p) * 2;
+                item_features(&x[r0 * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt, kChunk, ts, dens, tiles, sg);
+                item_features(&x[(r0 + 1) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt,
+                              std::max<uint32_t>(1, cnt % kChunk), ts, dens, tiles, sg);
+            }
         }
     }
     double ref_b = 0;
@@ -527,34 +534,39 @@ void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, do
         const uint32_t tiles = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
         const uint32_t ns = std::max<uint32_t>(1, (tiles + seg - 1) / seg);
         const uint32_t cnt = uint32_t(std::llround(ref_b * frac_[p]));
-        item_features(&x[(size_t(kTableSteps) * P * 2 + p) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt,
+        item_features(&x[(size_t(kSegChoices) * per_seg + p) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt,
                       std::min<uint32_t>(kChunk, std::max<uint32_t>(cnt, 1)), (tiles + ns - 1) / ns,
                       std::max(density_[p], 0.f), tiles, seg);
     }
     model_.predict(x.data(), rows, y.data(), st);
     const double ctas = double(std::max(sm_count, 1)) * 4.0;
-    table_ms_.assign(kTableSteps, 0.0);
-    for (int k = 0; k < kTableSteps; ++k) {
-        double cyc = 0;
-        for (uint32_t p = 0; p < P; ++p) {
-            const uint32_t tiles = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
-            const uint32_t ns = std::max<uint32_t>(1, (tiles + seg - 1) / seg);
-            const size_t r0 = (size_t(k) * P + p) * 2;
-            const uint32_t nf = nfull[size_t(k) * P + p], rm = rem[size_t(k) * P + p];
-            cyc += double(ns) * (nf * std::exp(double(y[r0])) + (rm ? std::exp(double(y[r0 + 1])) : 0.0));
+    table_ms_.assign(size_t(kSegChoices) * kTableSteps, 0.0);
+    for (int si = 0; si < kSegChoices; ++si) {
+        const uint32_t sg = kSegChoice[si];
+        for (int k = 0; k < kTableSteps; ++k) {
+            const uint32_t cnt_scale = 1u << k;
+            double cyc = 0, longest = 0;
+            for (uint32_t p = 0; p < P; ++p) {
+                const uint32_t tiles = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
+                const uint32_t ns = std::max<uint32_t>(1, (tiles + sg - 1) / sg);
+                const size_t r0 = size_t(si) * per_seg + (size_t(k) * P + p) * 2;
+                const uint32_t cnt = uint32_t(std::llround(double(cnt_scale) * frac_[p]));
+                const uint32_t nf = cnt / kChunk, rm = cnt % kChunk;
+                const double cf = std::exp(double(y[r0])), cr = rm ? std::exp(double(y[r0 + 1])) : 0.0;
+                cyc += double(ns) * (nf * cf + cr);
+                if (nf) longest = std::max(longest, cf);
+                if (rm) longest = std::max(longest, cr);
+            }
+            // item cycles are summed over the CTA's 8 warps
+            table_ms_[size_t(si) * kTableSteps + k] = std::max(cyc / ctas, longest) / 8.0 / clock_hz * 1e3;
         }
-        // item cycles are summed over the CTA's 8 warps
-        table_ms_[k] = cyc / 8.0 / ctas / clock_hz * 1e3;
     }
     // batch ms = fit0 + fit1 * kernel ms + fit2 * keys / 1e6: least squares
     // with non-negative coefficients (the best of the 7 subsets of terms
     // whose unconstrained solution is non-negative)
     double A[3][3] = {{0}}, B[3] = {0}, YY = 0;
     for (const auto &o : obs_) {
-        const double kb = std::log2(std::max(o[0], 1.0));
-        const int k0 = std::min(kTableSteps - 2, int(kb));
-        const double fr = std::min(1.0, kb - k0);
-        const double km = table_ms_[k0] * std::pow(table_ms_[k0 + 1] / std::max(table_ms_[k0], 1e-9), fr);
+        const double km = kernel_ms_locked(uint32_t(std::max(o[0], 1.0)), uint32_t(o[3]));
         const double v[3] = {1.0, km, o[2] / 1e6};
         for (int i = 0; i < 3; ++i) {
             for (int j = 0; j < 3; ++j) A[i][j] += v[i] * v[j];
@@ -606,7 +618,7 @@ void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, do
     std::copy(best, best + 3, fit_);
     // work-queue order: most expensive items first
     std::vector<float> cost(P);
-    for (uint32_t p = 0; p < P; ++p) cost[p] = y[size_t(kTableSteps) * P * 2 + p];
+    for (uint32_t p = 0; p < P; ++p) cost[p] = y[size_t(kSegChoices) * per_seg + p];
     order_.resize(P);
     std::iota(order_.begin(), order_.end(), 0u);
     std::stable_sort(order_.begin(), order_.end(), [&](uint32_t a, uint32_t b) { return cost[a] > cost[b]; });
@@ -617,23 +629,67 @@ std::vector<uint32_t> Scheduler::order() const {
     return order_;
 }
 
-double Scheduler::predict_batch_ms(uint32_t b) const {
-    std::lock_guard<std::mutex> lk(mtx_);
+// Predicted kernel ms of a batch of b queries at seg tiles per item (the
+// nearest candidate), interpolated between powers of two of b.
+double Scheduler::kernel_ms_locked(uint32_t b, uint32_t seg) const {
     if (table_ms_.empty() || b == 0) return 0.0;
+    int si = 0;
+    for (int i = 1; i < kSegChoices; ++i)
+        if (std::fabs(std::log2(double(kSegChoice[i]) / seg)) < std::fabs(std::log2(double(kSegChoice[si]) / seg))) si = i;
+    const double *tm = &table_ms_[size_t(si) * kTableSteps];
     const double kb = std::log2(double(b));
     const int k0 = std::min(kTableSteps - 2, int(kb));
     const double fr = std::min(1.0, kb - k0);
-    const double km = table_ms_[k0] * std::pow(table_ms_[k0 + 1] / std::max(table_ms_[k0], 1e-9), fr);
+    return tm[k0] * std::pow(tm[k0 + 1] / std::max(tm[k0], 1e-9), fr);
+}
+
+uint32_t Scheduler::best_seg_locked(uint32_t b) const {
+    uint32_t best = kSegChoice[0];
+    double best_ms = 1e300;
+    for (int i = 0; i < kSegChoices; ++i) {
+        const double ms = kernel_ms_locked(b, kSegChoice[i]);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = kSegChoice[i];
+        }
+    }
+    return best;
+}
+
+uint32_t Scheduler::best_seg(uint32_t b) const {
+    std::lock_guard<std::mutex> lk(mtx_);
+    return table_ms_.empty() ? 0u : best_seg_locked(b);
+}
+
+double Scheduler::model_batch_ms_locked(uint32_t b) const {
+    const double km = kernel_ms_locked(b, best_seg_locked(b));
     return fit_[0] + fit_[1] * km + fit_[2] * keys_per_query_ * b / 1e6;
 }
 
-uint32_t Scheduler::stable_batch(double rate_qps, uint32_t cap) const {
+double Scheduler::predict_batch_ms(uint32_t b) const {
+    std::lock_guard<std::mutex> lk(mtx_);
+    if (table_ms_.empty() || b == 0) return 0.0;
+    const int k = std::min(kTableSteps - 1, int(std::log2(double(b))));
+    return model_batch_ms_locked(b) * correction_[k];
+}
+
+void Scheduler::observe_batch(uint32_t b, double ms) {
+    std::lock_guard<std::mutex> lk(mtx_);
+    if (table_ms_.empty() || b == 0 || ms <= 0) return;
+    const double pred = model_batch_ms_locked(b);
+    if (pred <= 0) return;
+    const int k = std::min(kTableSteps - 1, int(std::log2(double(b))));
+    correction_[k] = 0.9 * correction_[k] + 0.1 * std::min(8.0, std::max(0.125, ms / pred));
+}
+
+uint32_t Scheduler::stable_batch(double rate_qps, uint32_t cap, int lanes) const {
     if (cap <= 1 || rate_qps <= 0) return 1;
-    // steps of 2^(1/4)
+    // steps of 2^(1/4); the lanes' batches run side by side, and the batch
+    // times were measured that way
     for (double b = 1; b < cap; b *= 1.189207115) {
         const uint32_t bi = uint32_t(b);
         const double ms = predict_batch_ms(bi);
-        if (ms > 0 && bi / ms * 1e3 >= 1.25 * rate_qps) return bi;
+        if (ms > 0 && lanes * bi / ms * 1e3 >= 1.25 * rate_qps) return bi;
     }
     return cap;
 }

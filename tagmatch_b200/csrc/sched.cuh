@@ -93,24 +93,41 @@ public:
     bool trained() const;
     // Partitions in descending order of predicted item cost.
     std::vector<uint32_t> order() const;
-    // Predicted milliseconds of a batch of b queries (0 when untrained).
+    // Predicted milliseconds of a batch of b queries at its best tiles per
+    // work item (0 when untrained).
     double predict_batch_ms(uint32_t b) const;
-    // Smallest batch (at most cap) whose predicted throughput, queries over
-    // predicted batch time, is at least 1.25 x the arrival rate: batches of
-    // that size keep up with the arrivals.
-    uint32_t stable_batch(double rate_qps, uint32_t cap) const;
+    // Tiles per work item with the lowest predicted kernel time for a batch
+    // of b queries (0 when untrained).
+    uint32_t best_seg(uint32_t b) const;
+    // A matched batch's measured milliseconds: corrects the predictions
+    // online, one factor per power-of-two batch size (moving average of
+    // measured over predicted).
+    void observe_batch(uint32_t b, double ms);
+    // Smallest batch (at most cap) whose predicted throughput -- lanes x
+    // queries over predicted batch time, the lanes' batches running side by
+    // side -- is at least 1.25 x the arrival rate: batches of that size keep
+    // up with the arrivals.
+    uint32_t stable_batch(double rate_qps, uint32_t cap, int lanes) const;
 
 private:
     void refresh_locked(const DevTable &t, uint32_t seg_tiles, int sm_count, double clock_hz, cudaStream_t st);
+    double kernel_ms_locked(uint32_t b, uint32_t seg) const;
+    uint32_t best_seg_locked(uint32_t b) const;
+    double model_batch_ms_locked(uint32_t b) const;
+    std::array<double, 19> correction_ = [] {
+        std::array<double, 19> c{};
+        c.fill(1.0);
+        return c;
+    }();
     mutable std::mutex mtx_;
     bool recording_ = false;
     std::vector<float> x_, t_;                 // samples: features [n][8], log warp-cycles [n]
     std::vector<float> density_, frac_;        // per partition: match density, routed queries per query
-    std::vector<std::array<double, 3>> obs_;   // batches: queries, measured ms, keys
+    std::vector<std::array<double, 4>> obs_;   // batches: queries, measured ms, keys, tiles per item
     double keys_per_query_ = 0;
     CostModel model_;
     std::vector<uint32_t> order_;
-    std::vector<double> table_ms_;             // predicted kernel ms for b = 2^k
+    std::vector<double> table_ms_;             // predicted kernel ms, [tiles-per-item choice][b = 2^k]
     double fit_[3] = {0, 1, 0};                // batch ms = fit0 + fit1 * kernel ms + fit2 * keys / 1e6
 };
 

@@ -10,11 +10,12 @@
 // Modes: "plain" = one request per device batch on one lane
 // (TM_FLUSH_SINGLE); "continuous" = all pending requests share the next
 // batch on either of two lanes (TM_FLUSH_IMMEDIATE); "learned" = continuous
-// batching with the learned scheduler's flush points (TM_FLUSH_LEARNED).
-// Before the first "learned" run the engine records timing samples while it
-// serves a calibration load in continuous mode (the first rate, calib=T
-// seconds), trains its cost model on the GPU and prints the training report
-// as a line with "mode": "learned-training".
+// batching with the learned scheduler's flush points and per-batch tiles
+// per work item (TM_FLUSH_LEARNED).  Before the first "learned" run the
+// engine records timing samples while it serves a calibration load in
+// continuous mode (the first and the last rate, calib=T seconds split over
+// five tiles per item values), trains its cost model on the GPU and prints the
+// training report as a line with "mode": "learned-training".
 //
 // usage: tagmatch_serve_bench [filters=N] [pool=Q] [seed=S] [maxp=P]
 //          [rates=r1,r2,...] [modes=plain,continuous,learned] [seconds=T]
@@ -191,9 +192,19 @@ int main(int argc, char **argv) {
         for (const std::string &mode : split(modes)) {
             int fm = mode == "plain" ? TM_FLUSH_SINGLE : mode == "learned" ? TM_FLUSH_LEARNED : TM_FLUSH_IMMEDIATE;
             if (mode == "learned" && !trained) {
-                // calibration: timing samples from continuous serving, then training
+                // calibration: timing samples from continuous serving at several
+                // tiles per work item (the model chooses among them), then training
                 tm_sched_record(e, 1);
-                if (!run(TM_FLUSH_IMMEDIATE, std::stod(split(rates).front()), calib, "calibration", false)) return 2;
+                const uint32_t seg0 = tm_get_tiles_per_item(e);
+                const double r_lo = std::stod(split(rates).front()), r_hi = std::stod(split(rates).back());
+                for (uint32_t sg : {32u, 128u, 512u, 2048u, 8192u}) {
+                    tm_set_tiles_per_item(e, sg);
+                    // small batches at the lowest rate, large ones at the highest
+                    if (!run(TM_FLUSH_IMMEDIATE, r_lo, calib / 10, "calibration", false) ||
+                        !run(TM_FLUSH_IMMEDIATE, r_hi, calib / 10, "calibration", false))
+                        return 2;
+                }
+                tm_set_tiles_per_item(e, seg0);
                 tm_sched_record(e, 0);
                 tm_sched_report rep{};
                 if (tm_sched_train(e, epochs, &rep) != TM_OK) {
