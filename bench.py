@@ -72,6 +72,10 @@ def parse():
     ap.add_argument("--serve-results", default="host,device")
     ap.add_argument("--latency-target-ms", type=int, default=25)
     ap.add_argument("--no-learned", action="store_true", help="skip the learned work-queue order comparison")
+    ap.add_argument("--no-small-partitions", action="store_true",
+                    help="config 2: skip the small-partition CPU backend comparison")
+    ap.add_argument("--small-threshold", type=int, default=1024, help="config 2: partitions below this many filters")
+    ap.add_argument("--small-queries", type=int, default=32768, help="config 2: queries of that comparison")
     ap.add_argument("--serve-seconds", type=float, default=3.0)
     return ap.parse_args()
 
@@ -416,12 +420,87 @@ def run_config2(args):
             par.append({"superset_fraction": s, "checked": p["checked"], "mismatches": p["mismatches"]})
         line["parity"] = {"checked": sum(p["checked"] for p in par), "mismatches": sum(p["mismatches"] for p in par),
                           "per_fraction": par, "seg_tiles": tm.get_tiles_per_item(), "device_batch": B}
+    if rank == 0 and world == 1 and not args.no_small_partitions:
+        line["small_partitions"] = small_partition_comparison(f, ko, k, qs[0.5], dqs[0.5], args, stream)
     if rank == 0:
         print(json.dumps(line), flush=True)
     tm.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def small_partition_comparison(f, ko, k, q, dq, args, stream):
+    """The reference's small-partition CPU backend (back_end.cc:496-517) as a
+    measured comparison, not a fallback: the partitions of the table below
+    --small-threshold filters, one batch of queries routed to them by mask;
+    the CPU restatement of that backend on all host cores against the GPU
+    engine on a table of the same filters; parity of per-query digests."""
+    import torch
+
+    from oracle import oracle
+    from tagmatch_b200 import TagMatch, balanced_partitioning
+    from tagmatch_b200.tagmatch import read_device
+    nq = min(q.shape[0], args.small_queries)
+    q = q[:nq]
+    part_of, masks, sizes = balanced_partitioning(f, MAX_P)
+    small = np.nonzero(sizes < args.small_threshold)[0]
+    if small.size == 0:
+        return {"partitions": 0}
+    is_small = np.zeros(sizes.size, dtype=bool)
+    is_small[small] = True
+    sel = np.nonzero(is_small[part_of])[0]
+    sel = sel[np.argsort(part_of[sel], kind="stable")]
+    remap = np.full(sizes.size, -1, dtype=np.int64)
+    remap[small] = np.arange(small.size)
+    part_off = np.zeros(small.size + 1, dtype=np.uint32)
+    np.add.at(part_off, remap[part_of[sel]] + 1, 1)
+    part_off = np.cumsum(part_off).astype(np.uint32)
+    fg = np.ascontiguousarray(f[sel])
+    lens = (ko[1:] - ko[:-1])[sel].astype(np.int64)
+    kg_off = np.zeros(sel.size + 1, dtype=np.uint32)
+    kg_off[1:] = np.cumsum(lens)
+    starts = ko[sel].astype(np.int64)
+    pos = np.repeat(starts - kg_off[:-1].astype(np.int64), lens) + np.arange(int(kg_off[-1]), dtype=np.int64)
+    kg = k[pos]
+    route_off, routed = oracle.route(masks[small], q)
+    pair_tests = int(np.sum((part_off[1:] - part_off[:-1]).astype(np.int64) * (route_off[1:] - route_off[:-1])))
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    cc, ch = oracle.cpu_backend(fg, part_off, kg_off, kg, q, route_off, routed, threads=cores)
+    cpu_s = time.perf_counter() - t0
+    tm = TagMatch()
+    tm.set_persistence(False)
+    tm.add_many(fg, kg_off, kg)
+    tm.consolidate(MAX_P, 1)
+    tm.match_batch_device(dq.data_ptr(), nq, stream=stream.cuda_stream)  # warm-up
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(3):
+        e0.record(stream)
+        po, pk, _ = tm.match_batch_device(dq.data_ptr(), nq, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    off = read_device(po, nq + 1, np.uint64)
+    samp = np.arange(0, nq, max(1, nq // 512))
+    bad = 0
+    for i in samp:
+        keys = read_device(pk + int(off[i]) * 4, int(off[i + 1] - off[i]), np.uint32)
+        c, h = oracle.digest(np.array([0, keys.size], dtype=np.uint64), keys)
+        bad += int(c[0] != cc[i] or h[0] != ch[i])
+    tm.close()
+    gpu_s = statistics.median(ms) / 1e3
+    return {"threshold_filters": args.small_threshold, "partitions": int(small.size), "filters": int(sel.size),
+            "queries": nq, "routed_pairs": int(routed.size), "filter_query_tests": pair_tests,
+            "cpu_backend": {"s": round(cpu_s, 3), "queries_per_s": round(nq / cpu_s, 1), "cores": cores,
+                            "tests_per_s": round(pair_tests / cpu_s, 1),
+                            "how": "oracle/oracle.c restatement of back_end.cc:496-517 (every filter of the "
+                                   "partition against every routed query), partitions over all host threads"},
+            "gpu": {"s": round(gpu_s, 5), "queries_per_s": round(nq / gpu_s, 1),
+                    "how": "tm_match_batch_device on a table of the same filters (re-partitioned by the engine)"},
+            "gpu_over_cpu": round(cpu_s / gpu_s, 1),
+            "parity": {"checked": int(samp.size), "mismatches": bad}}
 
 
 def run_ours(args):

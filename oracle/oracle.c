@@ -210,6 +210,83 @@ int oracle_match_digest(const uint32_t *filters, uint64_t n, const uint32_t *key
 }
 
 /* ------------------------------------------------------------------ */
+/* The reference's small-partition CPU backend (back_end.cc:496-517):  */
+/* for a partition below the size threshold, every filter is tested    */
+/* against every query routed to the partition on the CPU, and the     */
+/* matching filter's keys are appended to the query's output.  Here    */
+/* the partitions are split over threads; each thread reduces its      */
+/* queries' keys to (count, multiset hash) as match_digest does, and   */
+/* the per-thread sums are added at the end.                           */
+/*   filters [n][6] grouped by partition (part_off[np + 1]), key CSR    */
+/*   per filter; routed[route_off[p] .. route_off[p + 1]) the query     */
+/*   indices routed to partition p.                                     */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    const uint32_t *filters, *part_off, *key_off, *keys, *queries, *route_off, *routed;
+    uint64_t p0, p1, nq;
+    uint64_t *counts, *hashes; /* per thread, nq each */
+} backend_job_t;
+
+static void *backend_worker(void *arg) {
+    backend_job_t *j = (backend_job_t *)arg;
+    for (uint64_t p = j->p0; p < j->p1; ++p) {
+        for (uint32_t f = j->part_off[p]; f < j->part_off[p + 1]; ++f) {
+            const uint32_t *fw = j->filters + (uint64_t)f * W;
+            for (uint32_t r = j->route_off[p]; r < j->route_off[p + 1]; ++r) {
+                const uint32_t qi = j->routed[r];
+                if (subset_of(fw, j->queries + (uint64_t)qi * W)) {
+                    for (uint32_t k = j->key_off[f]; k < j->key_off[f + 1]; ++k) {
+                        j->hashes[qi] += fin64((uint64_t)j->keys[k] + 0x9E3779B97F4A7C15ull);
+                        j->counts[qi] += 1;
+                    }
+                }
+            }
+        }
+    }
+    return NULL;
+}
+
+int oracle_cpu_backend(const uint32_t *filters, const uint32_t *part_off, uint64_t np, const uint32_t *key_off,
+                       const uint32_t *keys, const uint32_t *queries, uint64_t nq, const uint32_t *route_off,
+                       const uint32_t *routed, uint64_t *counts, uint64_t *hashes, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if ((uint64_t)nthreads > np) nthreads = np ? (int)np : 1;
+    pthread_t *th = (pthread_t *)malloc(sizeof(pthread_t) * nthreads);
+    backend_job_t *jobs = (backend_job_t *)malloc(sizeof(backend_job_t) * nthreads);
+    uint64_t *cnt = (uint64_t *)calloc((size_t)nthreads * (nq ? nq : 1), sizeof(uint64_t));
+    uint64_t *hsh = (uint64_t *)calloc((size_t)nthreads * (nq ? nq : 1), sizeof(uint64_t));
+    /* partitions dealt to threads by routed pair work, in contiguous runs */
+    uint64_t total = 0;
+    for (uint64_t p = 0; p < np; ++p)
+        total += (uint64_t)(part_off[p + 1] - part_off[p]) * (route_off[p + 1] - route_off[p]);
+    uint64_t p = 0, acc = 0;
+    for (int t = 0; t < nthreads; ++t) {
+        backend_job_t b = {filters, part_off, key_off, keys, queries, route_off, routed, p, p, nq,
+                           cnt + (size_t)t * nq, hsh + (size_t)t * nq};
+        const uint64_t goal = total * (uint64_t)(t + 1) / (uint64_t)nthreads;
+        while (p < np && (acc < goal || t == nthreads - 1)) {
+            acc += (uint64_t)(part_off[p + 1] - part_off[p]) * (route_off[p + 1] - route_off[p]);
+            ++p;
+        }
+        b.p1 = p;
+        jobs[t] = b;
+        pthread_create(&th[t], NULL, backend_worker, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+    for (uint64_t q = 0; q < nq; ++q) {
+        uint64_t c = 0, h = 0;
+        for (int t = 0; t < nthreads; ++t) {
+            c += cnt[(size_t)t * nq + q];
+            h += hsh[(size_t)t * nq + q];
+        }
+        counts[q] = c;
+        hashes[q] = h;
+    }
+    free(cnt); free(hsh); free(th); free(jobs);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Balanced partitioning, restated from partitioning.cc.               */
 /*                                                                     */
 /* The reference runs a thread pool over a queue of candidates         */

@@ -43,6 +43,8 @@ def _load():
                                     u64p, ctypes.c_int]
         lib.oracle_match_digest.argtypes = [u32p, ctypes.c_uint64, u32p, u32p, u32p, ctypes.c_uint64, ctypes.c_int,
                                             u64p, u64p, ctypes.c_int]
+        lib.oracle_cpu_backend.argtypes = [u32p, u32p, ctypes.c_uint64, u32p, u32p, u32p, ctypes.c_uint64, u32p, u32p,
+                                           u64p, u64p, ctypes.c_int]
         lib.oracle_partition.restype = ctypes.c_int64
         lib.oracle_partition.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, u32p, u32p, ctypes.c_uint64]
         lib.oracle_subset_of.argtypes = [u32p, u32p]
@@ -102,6 +104,50 @@ def match_digest(filters, key_off, keys, queries, unique=False, threads=None):
     hashes = np.zeros(max(nq, 1), dtype=np.uint64)
     lib.oracle_match_digest(_p32(f), f.shape[0], _p32(ko), _p32(k), _p32(q), nq, 1 if unique else 0, _p64(counts),
                             _p64(hashes), threads)
+    return counts[:nq], hashes[:nq]
+
+
+def route(masks, queries, chunk=4096):
+    """Queries routed to each partition (mask subset of the query): CSR
+    (route_off [P + 1] uint32, routed query indices uint32)."""
+    m = np.ascontiguousarray(masks, dtype=np.uint32).reshape(-1, 6)
+    q = np.ascontiguousarray(queries, dtype=np.uint32).reshape(-1, 6)
+    lists = [[] for _ in range(m.shape[0])]
+    for q0 in range(0, q.shape[0], chunk):
+        qq = q[q0:q0 + chunk]
+        ok = np.ones((m.shape[0], qq.shape[0]), dtype=bool)
+        for w in range(6):
+            ok &= (m[:, w][:, None] & ~qq[:, w][None, :]) == 0
+        for p, qi in zip(*np.nonzero(ok)):
+            lists[p].append(q0 + qi)
+    off = np.zeros(m.shape[0] + 1, dtype=np.uint32)
+    off[1:] = np.cumsum([len(x) for x in lists])
+    routed = np.array([i for x in lists for i in x], dtype=np.uint32)
+    return off, routed
+
+
+def cpu_backend(filters, part_off, key_off, keys, queries, route_off, routed, threads=None):
+    """The reference's small-partition CPU backend (back_end.cc:496-517):
+    per partition, every filter against every routed query.  filters are
+    grouped by partition (part_off); returns digest (count, hash) arrays."""
+    lib = _load()
+    threads = threads or os.cpu_count() or 1
+    f = np.ascontiguousarray(filters, dtype=np.uint32).reshape(-1, 6)
+    po = np.ascontiguousarray(part_off, dtype=np.uint32)
+    ko = np.ascontiguousarray(key_off, dtype=np.uint32)
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    if k.size == 0:
+        k = np.zeros(1, dtype=np.uint32)
+    q = np.ascontiguousarray(queries, dtype=np.uint32).reshape(-1, 6)
+    ro = np.ascontiguousarray(route_off, dtype=np.uint32)
+    rt = np.ascontiguousarray(routed, dtype=np.uint32)
+    if rt.size == 0:
+        rt = np.zeros(1, dtype=np.uint32)
+    nq = q.shape[0]
+    counts = np.zeros(max(nq, 1), dtype=np.uint64)
+    hashes = np.zeros(max(nq, 1), dtype=np.uint64)
+    lib.oracle_cpu_backend(_p32(f), _p32(po), po.size - 1, _p32(ko), _p32(k), _p32(q), nq, _p32(ro), _p32(rt),
+                           _p64(counts), _p64(hashes), threads)
     return counts[:nq], hashes[:nq]
 
 
