@@ -746,25 +746,72 @@ __global__ void __launch_bounds__(kUniqThreads) k_unique_bitmap(const uint32_t *
     }
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) bm[i] = 0;
     __syncthreads();
-    for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+    // four key loads in flight per thread
+    constexpr uint32_t kU = 4;
+    uint64_t i = b + threadIdx.x;
+    for (; i + (kU - 1) * blockDim.x < e; i += kU * blockDim.x) {
+        uint32_t k[kU];
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) k[u] = keys[i + u * blockDim.x];
+#pragma unroll
+        for (uint32_t u = 0; u < kU; ++u) atomicOr(&bm[k[u] >> 5], 1u << (k[u] & 31));
+    }
+    for (; i < e; i += blockDim.x) {
         const uint32_t k = keys[i];
         atomicOr(&bm[k >> 5], 1u << (k & 31));
     }
     __syncthreads();
-    const uint32_t per = (words + blockDim.x - 1) / blockDim.x;
-    const uint32_t w0 = threadIdx.x * per, w1 = min(w0 + per, words);
+    // read-out in order: warp w takes words [w * per, (w + 1) * per), 32 at
+    // a time (lane l word l); a prefix sum over the lanes' popcounts places
+    // the round's keys, which the warp then writes 32 consecutive keys per
+    // step (each lane finds the word holding its key by a 5-step shuffle
+    // search, then the bit by halving popcounts), so the stores coalesce
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint32_t per = ((words + nwarps - 1) / nwarps + 31) & ~31u;
+    const uint32_t w0 = min(words, warp * per), w1 = min(words, w0 + per);
     uint32_t c = 0;
-    for (uint32_t w = w0; w < w1; ++w) c += __popc(bm[w]);
+    for (uint32_t w = w0 + lane; w < w1; w += 32) c += __popc(bm[w]);
+    c = __reduce_add_sync(kFull, c);
     uint32_t tot;
-    uint32_t pos = block_excl_scan<uint32_t>(c, tot);
+    uint32_t pos = block_excl_scan<uint32_t>(lane == 0 ? c : 0u, tot);
+    pos = __shfl_sync(kFull, pos, 0);  // this warp's first output position
     uint64_t d = b + pos;
-    for (uint32_t w = w0; w < w1; ++w) {
-        uint32_t x = bm[w];
-        while (x) {
-            const uint32_t bit = __ffs(x) - 1;
-            x &= x - 1;
-            ukeys[d++] = w * 32 + bit;
+    for (uint32_t r0 = w0; r0 < w1; r0 += 32) {
+        const uint32_t w = r0 + lane;
+        const uint32_t x = w < w1 ? bm[w] : 0u;
+        const uint32_t cnt = __popc(x);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int s = 1; s < 32; s <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, s);
+            if (lane >= (unsigned)s) incl += v;
         }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t owner = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
+                if (v <= j) owner += step;
+            }
+            const uint32_t oincl = __shfl_sync(kFull, incl, owner), ocnt = __shfl_sync(kFull, cnt, owner);
+            uint32_t ox = __shfl_sync(kFull, x, owner);
+            if (j < total) {
+                uint32_t rk = j - (oincl - ocnt), bit = 0;  // rank of the key's bit within the word
+#pragma unroll
+                for (int s = 16; s >= 1; s >>= 1) {
+                    const uint32_t lowc = __popc(ox & ((1u << s) - 1u));
+                    if (rk >= lowc) {
+                        rk -= lowc;
+                        ox >>= s;
+                        bit += s;
+                    }
+                }
+                ukeys[d + j] = (r0 + owner) * 32 + bit;
+            }
+        }
+        d += total;
     }
     if (threadIdx.x == 0) ucount[q] = tot;
 }
@@ -840,7 +887,16 @@ __global__ void k_compact(const uint32_t *__restrict__ ukeys, const uint64_t *__
     const uint32_t q = blockIdx.x;
     if (q >= nq) return;
     const uint64_t src = qoff[q], dst = uoff[q], n = uoff[q + 1] - uoff[q];
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) out[dst + i] = ukeys[src + i];
+    // four loads in flight per thread
+    uint64_t i = threadIdx.x;
+    for (; i + 3 * blockDim.x < n; i += 4 * blockDim.x) {
+        uint32_t v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) v[u] = ukeys[src + i + u * blockDim.x];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) out[dst + i + u * blockDim.x] = v[u];
+    }
+    for (; i < n; i += blockDim.x) out[dst + i] = ukeys[src + i];
 }
 
 // Copies na words at a, then nb words at b, into mapped pinned host memory
