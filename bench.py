@@ -573,11 +573,15 @@ def run_ours(args):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / kern_s / 1e9
     traffic = None
+    issue = None
     prof = os.path.join(ROOT, "profiles", "k_match_traffic.txt")
     if os.path.exists(prof):
         kv = dict(l.strip().split("=", 1) for l in open(prof) if "=" in l and not l.startswith("#"))
         # the captured case is smaller than a full launch; scale by queries
         traffic = round(float(kv["dram_bytes"]) * (st["queries"] / launches) / float(kv["queries_per_launch"]))
+        if "alu_pipe_frac" in kv:
+            issue = {"alu_pipe_frac": float(kv["alu_pipe_frac"]), "issue_active_frac": float(kv["issue_active_frac"]),
+                     "source": "ncu --set full of one 16,384-query launch (profiles/k_match_config1_small.md)"}
     int_ops = 6 * st["dense_tests"] / launches
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -585,7 +589,8 @@ def run_ours(args):
                 "kernel": "k_match (subset test)", "kernel_ms_per_launch": round(kern_s * 1e3, 3),
                 "alg_bytes_per_launch": int(alg_bytes),
                 "dense_word_tests_per_s": round(int_ops / kern_s / 1e12, 2),
-                "dense_word_tests_unit": "T/s (6 per routed (query, filter) pair, before tile pruning)"}
+                "dense_word_tests_unit": "T/s (6 per routed (query, filter) pair, before tile pruning)",
+                "binding": "instruction issue (integer ALU pipe); DRAM is not the limit", "issue": issue}
 
     line = {"metric": METRIC, "value": round(world * nq / (ms_max / 1e3), 1), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max, 3), "higher_is_better": True,

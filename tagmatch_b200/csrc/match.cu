@@ -287,7 +287,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
                                     cudaMemcpyDeviceToHost, st));
     }
     // ---- keys ----
-    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256 * kFillPerLane), unsigned(s.sm_count) * 16));
+    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], kFillThreads * kFillPerLane), unsigned(s.sm_count) * 16));
     // record-count readback, fill, key-total readback; each retry: match + readback
     bs.launches += 3 + scan_launches(nq) + 2 * uint32_t(bs.retries);
     exclusive_scan<uint32_t, uint64_t>(s.qkeys.p, s.qoff.p, nq, s.scr, st);
@@ -297,7 +297,7 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     s.keys.reserve(std::max<uint64_t>(total, 1));
     s.qcursor.reserve(nq);
     TM_CUDA(cudaMemsetAsync(s.qcursor.p, 0, nq * sizeof(uint32_t), st));
-    k_key_fill<<<gblocks, 256, 0, st>>>(s.recs.p, s.counters.p, t.slot_key_off.p, t.keys.p, s.qoff.p, s.qcursor.p, s.keys.p);
+    k_key_fill<<<gblocks, kFillThreads, 0, st>>>(s.recs.p, s.counters.p, t.slot_key_off.p, t.tile_keys.p, t.keys.p, s.qoff.p, s.qcursor.p, s.keys.p);
     TM_CHECK_LAUNCH();
     if (!unique) {
         TM_CUDA(cudaStreamSynchronize(st));

@@ -631,99 +631,149 @@ inline void launch_match(const MatchArgs &a, unsigned grid, cudaStream_t st) {
 #endif
 constexpr int kFillPerLane = TM_FILL_PER_LANE;
 
+constexpr int kFillThreads = 256;
+constexpr int kFillWarps = kFillThreads / 32;
+constexpr int kFillStep = 32 * kFillPerLane;  // records per warp step
+
+// Position of the k-th set bit (k from 0) of x, which has more than k set
+// bits: halving popcounts.
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t k) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const uint32_t lowc = __popc(x & ((1u << s) - 1u));
+        if (k >= lowc) {
+            k -= lowc;
+            x >>= s;
+            pos += s;
+        }
+    }
+    return pos;
+}
+
 // Copies every record's keys into its query's range (qoff).  Each record's
 // keys are reserved with one atomic on the query's cursor (qcursor, zeroed
-// by the caller).  A warp takes 2 x 32 records per step, so that the four
-// dependent load levels (record -> cursor and key start -> keys) each have
-// two requests in flight per lane (6 CTAs per SM).  A run of adjacent hit bits is one
-// contiguous key range of the tile's slots; the warp copies one run per
-// lane per round together, 32 keys per step: a prefix sum over the lanes'
-// run lengths, and for key j of the round a 5-step shuffle search for the
-// lane that owns it.  Single-run records (the usual case) take one round;
-// the further runs of the others take further rounds, so no lane copies
-// keys on its own.
-__global__ void __launch_bounds__(256, TM_FILL_MIN_CTAS) k_key_fill(const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
-                                                  const uint32_t *__restrict__ slot_key_off, const uint32_t *__restrict__ tkeys,
-                                                  const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor,
-                                                  uint32_t *__restrict__ out) {
+// by the caller).  The table keeps keys in slot order, so each run of
+// adjacent hit bits [lo, hi) of a record's mask is the key range
+// [o[lo], o[hi]) of the tile's slot offsets o.  A warp takes 32 x
+// kFillPerLane records per step and numbers all their runs (a prefix sum
+// over the lanes' run counts); lane i of a batch then takes run 32 b + i:
+// a 5-step shuffle search for the lane whose records hold it, the record
+// from shared memory, the run's first bit by halving popcounts, its key
+// range from the slot offsets, and its place in the record's output from
+// the keys of the hit bits below it (the tile's key-count planes).  The
+// warp copies the batch's runs together, 32 keys per step (a prefix sum
+// over the run lengths and, for key j, a 5-step search for the run that
+// owns it), so the stores coalesce and a record with several runs costs no
+// extra pass over the warp.
+__global__ void __launch_bounds__(kFillThreads, TM_FILL_MIN_CTAS) k_key_fill(
+    const HitRec *__restrict__ recs, const unsigned long long *__restrict__ counters,
+    const uint32_t *__restrict__ slot_key_off, const TileKeys *__restrict__ tile_keys, const uint32_t *__restrict__ tkeys,
+    const uint64_t *__restrict__ qoff, uint32_t *__restrict__ qcursor, uint32_t *__restrict__ out) {
+    // per warp and record of the step: tile, hit mask, keys, runs of the
+    // lane's earlier records; and the record's first output position
+    __shared__ uint4 s_rec[kFillWarps][kFillStep];
+    __shared__ unsigned long long s_dst[kFillWarps][kFillStep];
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned long long n = counters[1];
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x >> 5);
-    const unsigned long long wid = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    constexpr unsigned kStep = 32 * kFillPerLane;
-    for (unsigned long long base = wid * kStep; base < n; base += warps * kStep) {
+    const unsigned long long warps = (unsigned long long)gridDim.x * kFillWarps;
+    const unsigned long long wid = (unsigned long long)blockIdx.x * kFillWarps + warp;
+    for (unsigned long long base = wid * kFillStep; base < n; base += warps * kFillStep) {
         HitRec r[kFillPerLane];
 #pragma unroll
         for (int j = 0; j < kFillPerLane; ++j) {
             const unsigned long long i = base + j * 32 + lane;
             r[j] = i < n ? recs[i] : HitRec{kPadQuery, 0u, 0u, 0u};
         }
-        uint32_t nk[kFillPerLane], src[kFillPerLane];
-        uint64_t dst[kFillPerLane];
-        bool single[kFillPerLane];
+        uint32_t nruns = 0;
+        unsigned long long dst[kFillPerLane];
 #pragma unroll
         for (int j = 0; j < kFillPerLane; ++j) {
-            nk[j] = r[j].query == kPadQuery ? 0u : r[j].nkeys;
-            dst[j] = 0;
-            if (nk[j]) dst[j] = qoff[r[j].query] + atomicAdd(&qcursor[r[j].query], nk[j]);
+            const bool live = r[j].query != kPadQuery && r[j].nkeys != 0;
+            const uint32_t m = live ? r[j].mask : 0u;
+            dst[j] = live ? qoff[r[j].query] + atomicAdd(&qcursor[r[j].query], r[j].nkeys) : 0ull;
+            s_rec[warp][j * 32 + lane] = make_uint4(r[j].tile, m, live ? r[j].nkeys : 0u, nruns);
+            nruns += __popc(m & ~(m << 1));  // run starts
         }
+        uint32_t incl = nruns;
 #pragma unroll
-        for (int j = 0; j < kFillPerLane; ++j) {
-            const uint32_t lo = nk[j] ? uint32_t(__ffs(r[j].mask)) - 1 : 0u;
-            const uint32_t run = r[j].mask >> lo;
-            single[j] = nk[j] && (run & (run + 1)) == 0;  // one run of adjacent bits
-            src[j] = single[j] ? __ldg(&slot_key_off[size_t(r[j].tile) * kTile + lo]) : 0u;
+        for (int s = 1; s < 32; s <<= 1) {
+            const uint32_t v = __shfl_up_sync(kFull, incl, s);
+            if (lane >= (unsigned)s) incl += v;
         }
+        const uint32_t total = __shfl_sync(kFull, incl, 31);
+        const uint32_t excl = incl - nruns;
+        __syncwarp();
+        for (uint32_t rb = 0; rb < total; rb += 32) {
+            const uint32_t ri = rb + lane;
+            uint32_t owner = 0;  // first lane whose inclusive run count exceeds ri
 #pragma unroll
-        for (int j = 0; j < kFillPerLane; ++j) {
-            // the warp copies one run of adjacent hit bits per lane per round
-            // (a single-run record in one round; the runs of other records
-            // in further rounds), 32 keys per step
-            const uint32_t *o = slot_key_off + size_t(r[j].tile) * kTile;
-            uint64_t m = nk[j] ? r[j].mask : 0u;
-            uint64_t d = dst[j];
-            bool first = true;
-            while (__any_sync(kFull, m != 0)) {
-                uint32_t len = 0, s = 0;
-                if (m) {
-                    const int lo = __ffsll(m) - 1;
-                    const uint64_t filled = m + (1ull << lo);  // the carry clears the run and sets bit hi
-                    const int hi = __ffsll(filled & ~m) - 1;
-                    if (first && single[j]) {
-                        s = src[j];
-                        len = nk[j];
-                    } else {
-                        s = o[lo];
-                        len = o[hi] - s;
-                    }
-                    m &= filled;
-                }
-                first = false;
-                uint32_t incl = len;
+            for (int s = 16; s >= 1; s >>= 1) {
+                const uint32_t v = __shfl_sync(kFull, incl, owner + s - 1);
+                if (v <= ri) owner += s;
+            }
+            const uint32_t oexcl = __shfl_sync(kFull, excl, owner);
+            const bool have = ri < total;
+            uint32_t slot = owner, src = 0, end = 0, below = 0, t = 0, nk = 0;
+            bool last = true;
+            TileKeys tk{{0u, 0u, 0u}, 0u};
+            if (have) {
+                const uint32_t k = ri - oexcl;  // run number within the owner lane's records
+                // its record: the last whose earlier-run count is <= k
 #pragma unroll
-                for (int step = 1; step < 32; step <<= 1) {
-                    const uint32_t v = __shfl_up_sync(kFull, incl, step);
-                    if (lane >= (unsigned)step) incl += v;
-                }
-                const uint32_t total = __shfl_sync(kFull, incl, 31);
-                const uint32_t start = incl - len;  // this lane's first key among the round's
-                for (uint32_t j0 = 0; j0 < total; j0 += 32) {
-                    const uint32_t k = j0 + lane;
-                    // owner: the first lane whose inclusive count exceeds k
-                    uint32_t owner = 0;
+                for (int jj = 1; jj < kFillPerLane; ++jj)
+                    if (s_rec[warp][jj * 32 + owner].w <= k) slot = jj * 32 + owner;
+                const uint4 rc = s_rec[warp][slot];
+                const uint32_t m = rc.y;
+                t = rc.x;
+                nk = rc.z;
+                const uint32_t lo = nth_set_bit(m & ~(m << 1), k - rc.w);
+                const uint32_t hi = lo + uint32_t(__ffsll(~((unsigned long long)m >> lo))) - 1u;
+                const uint32_t *o = slot_key_off + size_t(t) * kTile;
+                below = m & ((1u << lo) - 1u);  // hit bits of the earlier runs
+                last = hi >= 32u || (m >> hi) == 0u;
+                src = o[lo];
+                if (!last) end = o[hi];
+                if (below) tk = tile_keys[t];
+            }
+            if (rb == 0) {
+                // the cursor atomics' results, published once the first
+                // batch's offset loads are in flight
 #pragma unroll
-                    for (int step = 16; step >= 1; step >>= 1) {
-                        const uint32_t v = __shfl_sync(kFull, incl, owner + step - 1);
-                        if (v <= k) owner += step;
-                    }
-                    const uint32_t ostart = __shfl_sync(kFull, start, owner);
-                    const uint32_t osrc = __shfl_sync(kFull, s, owner);
-                    const uint64_t odst = __shfl_sync(kFull, d, owner);
-                    if (k < total) out[odst + (k - ostart)] = tkeys[osrc + (k - ostart)];
+                for (int j = 0; j < kFillPerLane; ++j) s_dst[warp][j * 32 + lane] = dst[j];
+                __syncwarp();
+            }
+            uint32_t len = 0;
+            unsigned long long d = 0;
+            if (have) {
+                const uint32_t bk = below ? mask_keys(tk, below, slot_key_off, t) : 0u;
+                len = last ? nk - bk : end - src;
+                d = s_dst[warp][slot] + bk;
+            }
+            // the batch's runs, copied together
+            uint32_t kin = len;
+#pragma unroll
+            for (int s = 1; s < 32; s <<= 1) {
+                const uint32_t v = __shfl_up_sync(kFull, kin, s);
+                if (lane >= (unsigned)s) kin += v;
+            }
+            const uint32_t keys = __shfl_sync(kFull, kin, 31);
+            const uint32_t start = kin - len;
+            for (uint32_t j0 = 0; j0 < keys; j0 += 32) {
+                const uint32_t kk = j0 + lane;
+                uint32_t ro = 0;  // first lane whose inclusive key count exceeds kk
+#pragma unroll
+                for (int s = 16; s >= 1; s >>= 1) {
+                    const uint32_t v = __shfl_sync(kFull, kin, ro + s - 1);
+                    if (v <= kk) ro += s;
                 }
-                d += len;
+                const uint32_t ostart = __shfl_sync(kFull, start, ro);
+                const uint32_t osrc = __shfl_sync(kFull, src, ro);
+                const unsigned long long odst = __shfl_sync(kFull, d, ro);
+                if (kk < keys) out[odst + (kk - ostart)] = tkeys[osrc + (kk - ostart)];
             }
         }
+        __syncwarp();  // the shared entries are rewritten by the next step
     }
 }
 

@@ -207,7 +207,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
 
     // keys
     ar.trim(recs + hc[1]);
-    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], 256 * kFillPerLane), unsigned(sms) * 16));
+    const unsigned gblocks = std::max(1u, std::min(blocks_for(hc[1], kFillThreads * kFillPerLane), unsigned(sms) * 16));
     uint64_t *key_off = unique ? qoff : d_out_offsets;
     scan_fixed<uint32_t, uint64_t>(qkeys, key_off, nq, sums, offs, st);
     uint64_t total = 0;
@@ -217,7 +217,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
         *n_keys = total;
         if (total > capacity)
             throw Error(TM_ERR_CAPACITY, "output key buffer too small: " + std::to_string(total) + " keys needed");
-        k_key_fill<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, t.keys.p, d_out_offsets, qcursor, d_out_keys);
+        k_key_fill<<<gblocks, kFillThreads, 0, st>>>(recs, counters, t.slot_key_off.p, t.tile_keys.p, t.keys.p, d_out_offsets, qcursor, d_out_keys);
         TM_CHECK_LAUNCH();
         TM_CUDA(cudaStreamSynchronize(st));
         return;
@@ -232,7 +232,7 @@ void match_batch_noalloc(const DevTable &t, const uint32_t *d_queries, uint32_t 
     uint32_t *ukeys = std::max<uint64_t>(total, 1) * sizeof(uint32_t) <= hc[1] * sizeof(HitRec)
                           ? reinterpret_cast<uint32_t *>(recs)
                           : ar.take<uint32_t>(std::max<uint64_t>(total, 1), "match_unique keys");
-    k_key_fill<<<gblocks, 256, 0, st>>>(recs, counters, t.slot_key_off.p, t.keys.p, qoff, qcursor, keys);
+    k_key_fill<<<gblocks, kFillThreads, 0, st>>>(recs, counters, t.slot_key_off.p, t.tile_keys.p, t.keys.p, qoff, qcursor, keys);
     TM_CHECK_LAUNCH();
     if (bitmap) {
         k_unique_bitmap<<<nq, kUniqThreads, bitmap_words * 4, st>>>(keys, qoff, uint32_t(bitmap_words), ukeys, ucount);
