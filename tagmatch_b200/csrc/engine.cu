@@ -513,7 +513,9 @@ void Engine::worker_loop(int dev, int lane) {
                         // (predicted queries per ms of batch time), or when the
                         // oldest request's wait plus the batch's predicted time
                         // reaches half the latency target; otherwise wait for
-                        // more requests
+                        // more requests.  Below the predicted capacity (a stable
+                        // batch under the cap exists) a device with no batch on
+                        // it does not wait: waiting would only leave it idle.
                         const uint64_t bq = std::max<uint64_t>(1, memory_budget_.load() / std::max<uint64_t>(1, bytes_per_query_.load()));
                         const uint32_t cap = uint32_t(std::min<uint64_t>(batch_limit_, bq));
                         const uint32_t b0 = uint32_t(std::min<uint64_t>(pending_queries_, cap));
@@ -522,7 +524,7 @@ void Engine::worker_loop(int dev, int lane) {
                         const double age = std::chrono::duration<double, std::milli>(now - pending_.front()->arrived).count();
                         const double budget = 0.5 * latency_target_ms_.load();
                         const uint32_t need = sched_.stable_batch(arrival_qps_, cap, kLanes);
-                        if (b0 >= need || age + t0 >= budget) break;
+                        if (b0 >= need || age + t0 >= budget || (d.busy_lanes == 0 && need < cap)) break;
                         double wait_ms = budget - age - t0;
                         if (arrival_qps_ > 0) wait_ms = std::min(wait_ms, 1e3 * double(need - b0) / arrival_qps_);
                         q_cv_.wait_until(lk, now + std::chrono::microseconds(int64_t(1e3 * wait_ms) + 1));
@@ -561,11 +563,13 @@ void Engine::worker_loop(int dev, int lane) {
             pending_queries_ -= total;
             if (!pending_.empty()) oldest_ = std::chrono::steady_clock::now();
             in_flight_ += total;
+            ++d.busy_lanes;
         }
         run_pieces(d, ln, pieces, unique);
         {
             std::lock_guard<std::mutex> lk(q_mtx_);
             in_flight_ -= total;
+            --d.busy_lanes;
         }
         done_cv_.notify_all();
         q_cv_.notify_all();

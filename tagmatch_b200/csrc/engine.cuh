@@ -229,6 +229,7 @@ private:
         HostLane host[kHostLanes];  // synchronous host-buffer pipeline
         void *noalloc_scratch = nullptr;  // device address of the no-allocation array (looked up once)
         Lane lanes[kLanes];         // asynchronous matcher lanes
+        int busy_lanes = 0;         // lanes with a batch on this device (under q_mtx_)
     };
     void build_device_table(Device &d);
     // before / after every batch: work-queue order and timing record

@@ -45,3 +45,20 @@ def groups_from_assignment(partition_of, n_parts):
     for i, p in enumerate(partition_of):
         groups[int(p)].append(i)
     return sorted(tuple(g) for g in groups)
+
+
+def wide_key_lists(n, seed):
+    """Key lists for n filters in which about 10% of the filters hold 8..40
+    keys (the rest 1..7), unique and sorted per filter: CSR (key_offsets,
+    keys).  Counts of 8 or more take the slot-offset path of the matcher's
+    per-tile key-count planes."""
+    rng = np.random.default_rng(seed)
+    counts = rng.integers(1, 8, size=n)
+    wide = rng.random(n) < 0.1
+    counts[wide] = rng.integers(8, 41, size=int(wide.sum()))
+    ko = np.zeros(n + 1, dtype=np.uint32)
+    ko[1:] = np.cumsum(counts)
+    keys = np.empty(int(ko[-1]), dtype=np.uint32)
+    for i in range(n):
+        keys[ko[i]:ko[i + 1]] = np.sort(rng.choice(65536, size=int(counts[i]), replace=False))
+    return ko, keys

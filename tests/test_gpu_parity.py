@@ -13,7 +13,8 @@ from tagmatch_b200 import TagMatch, TagMatchError, balanced_partitioning, build,
 from tagmatch_b200 import _native
 from tagmatch_b200.tagmatch import filter_from_bits, filter_from_string
 from tests.conftest import golden
-from tests.helpers import assert_same_multisets, groups_from_assignment, load_partitions_golden, read_fixtures
+from tests.helpers import (assert_same_multisets, groups_from_assignment, load_partitions_golden, read_fixtures,
+                           wide_key_lists)
 
 pytestmark = pytest.mark.gpu
 
@@ -154,6 +155,18 @@ def test_single_bit_and_nested_filters():
             off, keys = tm.match_batch(ones, unique=True)
             assert keys.tolist() == list(range(192))
             tm.close()
+
+
+@pytest.mark.parametrize("max_p", [65536, 500])
+def test_wide_key_counts_and_split_hit_runs(max_p):
+    """Filters with 8..40 keys beside filters with 1..7, dense queries (so
+    that a tile's hit mask often has several runs of adjacent bits): the
+    key totals and the gather's run offsets take the slot offsets wherever
+    a run or the bits below it touch a filter with 8 keys or more."""
+    f, _, _ = workload.generate_filters(30000, 61)
+    ko, k = wide_key_lists(f.shape[0], 61)
+    q = workload.generate_queries(800, f, 61, superset_fraction=0.9)
+    check_against_oracle(f, ko, k, q, max_p)
 
 
 def test_many_queries_one_partition_chunks():

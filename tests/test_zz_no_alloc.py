@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from tagmatch_b200 import TagMatch, _native, workload
+from tests.helpers import wide_key_lists
 
 pytestmark = pytest.mark.gpu
 
@@ -81,12 +82,14 @@ def _same(unique, off, keys, ref_off, ref_keys):
             assert np.array_equal(a, b)
 
 
-# (filters, seed, max partition size, queries, key remap): the first case
-# has few partitions; the second more than one scan block (2,048) of
+# (filters, seed, max partition size, queries, keys): the first case has
+# few partitions; the second more than one scan block (2,048) of
 # partitions; the third a batch of 4,096 queries (two scan blocks of
 # per-query counts) and keys above the 48 KB bitmap of match_unique, so
-# that it takes the sort path.
-CASES = [(200_000, 51, 65536, 1500, False), (200_000, 52, 128, 512, False), (200_000, 53, 65536, 4096, True)]
+# that it takes the sort path; the fourth filters with 8..40 keys beside
+# filters with 1..7 (the slot-offset path of the key counts and gather).
+CASES = [(200_000, 51, 65536, 1500, "plain"), (200_000, 52, 128, 512, "plain"), (200_000, 53, 65536, 4096, "big"),
+         (50_000, 54, 65536, 1024, "wide")]
 
 
 @pytest.mark.parametrize("case", range(len(CASES)))
@@ -96,10 +99,13 @@ def test_noalloc_matches_allocating_entry_point(case, unique):
     torch.cuda.init()
     rt = _cudart()
     lib = _native.load()
-    nf, seed, max_p, n, big_keys = CASES[case]
+    nf, seed, max_p, n, key_kind = CASES[case]
     f, ko, k = workload.generate_filters(nf, seed)
+    big_keys = key_kind == "big"
     if big_keys:
         k = (k.astype(np.uint64) * 977 + 400_000).astype(np.uint32)
+    elif key_kind == "wide":
+        ko, k = wide_key_lists(nf, seed)
     q = workload.generate_queries(n, f, seed)
     tm = _engine(f, ko, k, max_p)
     info = tm.table_info()
