@@ -203,9 +203,10 @@ void match_batch(const DevTable &t, const uint32_t *d_queries, uint32_t nq, bool
     for (uint32_t pos = 0; pos < P; ++pos) {
         const uint32_t p = ordered ? s.part_order[pos] : pos;
         s.h_item_off[pos] = items;
-        const uint32_t nc = (s.h_part_count[p] + kChunk - 1) / kChunk;
+        // an item: kItemChunks chunks of the partition x one tile segment
+        const uint32_t ng = (s.h_part_count[p] + kItemQueries - 1) / kItemQueries;
         const uint32_t nt = t.h_part_tiles[p + 1] - t.h_part_tiles[p];
-        items += nc * ((nt + s.seg_tiles - 1) / s.seg_tiles);
+        items += ng * ((nt + s.seg_tiles - 1) / s.seg_tiles);
     }
     s.h_chunk_off[P] = chunks;
     s.h_item_off[P] = items;

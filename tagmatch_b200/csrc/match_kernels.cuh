@@ -13,7 +13,7 @@ constexpr int kRouteThreads = 256;
 constexpr int kMatchThreads = 256;
 constexpr int kMatchWarps = kMatchThreads / 32;
 constexpr int kWarpRecs = 64;  // staged hit records per warp (1 KB)
-constexpr int kQuad = 4;       // tiles a warp selects candidates for at once
+constexpr int kQuad = 2;       // tiles a warp selects candidates for at once (for both chunks of its item)
 constexpr uint32_t kMaxRouteParts = 1536;  // partition masks per routing window (48 KB of shared memory)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
@@ -229,16 +229,18 @@ struct __align__(128) Stage {
 
 // Shared memory of one matcher CTA (dynamic; ~51 KB, 4 CTAs per SM).
 struct MatchSmem {
-    Stage st[2];
+    Stage st[kItemChunks];                               // the item's chunks
     HitRec rec[kMatchWarps][kWarpRecs];                  // staged hit records per warp
-    uint8_t list[kMatchWarps][kQuad][kChunk + 8];        // candidate lists (query index in the chunk) per warp and tile
-    TileKeys tk[kMatchWarps][kQuad];                     // key-count planes of the warp's four tiles
+    // candidate lists per warp and tile: the first chunk's candidates, then
+    // the second's (query index in its chunk), padded to a multiple of 4
+    uint8_t list[kMatchWarps][kQuad][kItemQueries + 8];
+    TileKeys tk[kMatchWarps][kQuad];                     // key-count planes of the warp's tiles
     uint4 tf[kMatchWarps][kWords][kTile / 4];            // a warp's tile: word k of filters 4 g .. 4 g + 3
-    uint64_t full[2], empty[2];
-    uint32_t item[2];
+    uint64_t full, empty;
+    uint32_t item;
     int fail;
-    // thread 0's record of the copies in flight (bit s: stage s), with the
-    // parity of the phase that completes each
+    // thread 0's record of a copy in flight, with the parity of the phase
+    // that completes it
     uint32_t inflight, inflight_par;
 };
 
@@ -256,8 +258,11 @@ __device__ __forceinline__ void flush_recs(HitRec *buf, uint32_t n, const MatchA
     __syncwarp();
 }
 
+// A work item: kItemChunks consecutive 256-query chunks of one partition
+// (nq[c] queries in chunk c, 0 past the partition's last chunk) against one
+// segment of its tiles.
 struct ItemRef {
-    uint32_t p, qbase, nq, tb, te, zchunk;
+    uint32_t p, qbase, nq[kItemChunks], tb, te, zchunk;
 };
 
 __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
@@ -273,45 +278,60 @@ __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
     r.p = lo;
     const uint32_t pq = a.part_count[lo];
     const uint32_t nchunks = (pq + kChunk - 1) / kChunk;
-    const uint32_t chunk = local % nchunks, seg = local / nchunks;
-    r.qbase = a.part_off[lo] + chunk * kChunk;
-    r.nq = min((uint32_t)kChunk, pq - chunk * kChunk);
+    const uint32_t ngroups = (nchunks + kItemChunks - 1) / kItemChunks;
+    const uint32_t group = local % ngroups, seg = local / ngroups;
+    const uint32_t c0 = group * kItemChunks;
+    r.qbase = a.part_off[lo] + c0 * kChunk;
+#pragma unroll
+    for (int c = 0; c < kItemChunks; ++c)
+        r.nq[c] = c0 + c < nchunks ? min((uint32_t)kChunk, pq - (c0 + c) * kChunk) : 0u;
     r.tb = a.part_tile_begin[lo] + seg * a.seg_tiles;
     r.te = min(r.tb + a.seg_tiles, a.part_tile_begin[lo + 1]);
-    r.zchunk = a.chunk_off[lo] + chunk;
+    r.zchunk = a.chunk_off[lo] + c0;
     return r;
 }
 
-// Thread 0: claim the next item and start its copy into stage `buf`; the
-// item id is published through the full barrier's phase completion.
-// Returns whether a copy is in flight.
-__device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, MatchSmem &S, int buf) {
+// Thread 0: claim the next item and start the copies of its chunks' query
+// records and slices; the item id is published through the full barrier's
+// phase completion.  Returns whether copies are in flight.
+__device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, MatchSmem &S) {
     const uint32_t item = uint32_t(atomicAdd(&a.counters[0], 1ull));
-    S.item[buf] = item;
+    S.item = item;
     if (item < total) {
         const ItemRef r = locate(a, item);
-        const uint32_t qbytes = r.nq * kQueueWords * sizeof(uint32_t);
+        uint32_t bytes = 0;
+#pragma unroll
+        for (int c = 0; c < kItemChunks; ++c)
+            if (r.nq[c]) bytes += r.nq[c] * kQueueWords * sizeof(uint32_t) + kSliceWords * sizeof(uint32_t);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&S.full[buf], qbytes + kSliceWords * sizeof(uint32_t));
-        tma_bulk_g2s(S.st[buf].q, a.queue + size_t(r.qbase) * kQueueWords, qbytes, &S.full[buf]);
-        tma_bulk_g2s(S.st[buf].z, a.slices + size_t(r.zchunk) * kSliceWords, kSliceWords * sizeof(uint32_t), &S.full[buf]);
+        mbar_expect_tx(&S.full, bytes);
+#pragma unroll
+        for (int c = 0; c < kItemChunks; ++c) {
+            if (!r.nq[c]) continue;
+            tma_bulk_g2s(S.st[c].q, a.queue + (size_t(r.qbase) + size_t(c) * kChunk) * kQueueWords,
+                         r.nq[c] * kQueueWords * sizeof(uint32_t), &S.full);
+            tma_bulk_g2s(S.st[c].z, a.slices + (size_t(r.zchunk) + c) * kSliceWords, kSliceWords * sizeof(uint32_t),
+                         &S.full);
+        }
         return true;
     }
-    mbar_arrive(&S.full[buf]);  // nothing to copy: complete the phase so consumers see the end
+    mbar_arrive(&S.full);  // nothing to copy: complete the phase so consumers see the end
     return false;
 }
 
-// The subset test.  Persistent CTAs take work items (partition, 256-query
-// chunk, segment of the partition's tiles) from an atomic counter; thread 0
-// stages each item's query records and slices with bulk TMA copies into one
-// of two buffers while the CTA matches the other.  Each warp takes four
+// The subset test.  Persistent CTAs take work items (partition, two
+// consecutive 256-query chunks of its queue, segment of its tiles) from an
+// atomic counter; thread 0 stages the item's query records and slices with
+// bulk TMA copies into the CTA's two chunk buffers.  Each warp takes two
 // tiles (<= 32 filters each) at a time:
-//  * selection, for the four tiles at once: the tile's 8 selector bits
-//    (bits every member holds); lane l ORs the "lacks bit" slices of 32-query
-//    word l & 7 for tile l >> 3, so a query that lacks any of them is
-//    dropped; the remaining candidates go to the tile's list (one byte per
-//    query, placed by a prefix sum over the tile's 8 words);
-// then, tile by tile:
+//  * selection, for both tiles and both chunks at once: the tile's 8
+//    selector bits (bits every member holds); lane l ORs the "lacks bit"
+//    slices of 32-query word l & 7 of chunk (l >> 3) & 1 for tile l >> 4,
+//    so a query that lacks any of them is dropped; the remaining candidates
+//    go to the tile's list (one byte per query: the first chunk's, then the
+//    second's, placed by a prefix sum over the tile's 16 words);
+// then, tile by tile, over the candidates of both chunks together (one pass
+// over the tile's filters for 512 queries: fuller passes and trips):
 //  * many candidates: one candidate query per lane, the tile's filters read
 //    from shared memory (one broadcast 128-bit load gives word k of four
 //    filters): 6 LOP3 per (query, filter), the lane's hit mask over the tile
@@ -332,25 +352,19 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     MatchSmem &S = *reinterpret_cast<MatchSmem *>(smem_raw);
     const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t total = a.item_off[a.n_parts];
-    if (tid < 2 * kQueueWords) {
+    if (tid < kItemChunks * kQueueWords) {
         const uint32_t k = tid % kQueueWords;
         S.st[tid / kQueueWords].q[kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
     }
     if (tid == 0) {
-        mbar_init(&S.full[0], 1);
-        mbar_init(&S.full[1], 1);
-        mbar_init(&S.empty[0], kMatchWarps);
-        mbar_init(&S.empty[1], kMatchWarps);
+        mbar_init(&S.full, 1);
+        mbar_init(&S.empty, kMatchWarps);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         S.fail = 0;
-    }
-    __syncthreads();
-    // thread 0 keeps track of the copies in flight (stage, wait parity), so
-    // that no copy still targets this CTA's shared memory when it exits
-    if (tid == 0) {
-        S.inflight = produce(a, total, S, 0) ? 1u : 0u;
+        S.inflight = 0;
         S.inflight_par = 0;
     }
+    __syncthreads();
     uint32_t w_tiles = 0, w_passes = 0, w_cand = 0, w_trips = 0, w_items = 0, w_groups = 0, w_lanes = 0, w_small = 0;
     uint32_t wn = 0;      // records staged by this warp (warp-uniform)
     uint32_t w_recs = 0;  // records this warp has produced (warp-uniform)
@@ -358,29 +372,29 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     const uint32_t lane_lt = (1u << lane) - 1u;
     uint32_t *tfw = reinterpret_cast<uint32_t *>(S.tf[warp]);
     for (uint32_t it = 0;; ++it) {
-        const int b = it & 1;
-        // prefetch the next item into the other stage once every warp has
-        // released it (it held item it - 1)
+        // stage the next item once every warp has released the buffers
+        // (they held item it - 1); thread 0 keeps track of the copies in
+        // flight, so that none still targets this CTA's shared memory when
+        // it exits
         if (tid == 0) {
             bool ok = true;
-            if (it >= 1) ok = mbar_wait(&S.empty[b ^ 1], ((it - 1) >> 1) & 1);
+            if (it >= 1) ok = mbar_wait(&S.empty, (it - 1) & 1);
             if (ok) {
-                const uint32_t bit = 1u << (b ^ 1);
-                S.inflight = produce(a, total, S, b ^ 1) ? S.inflight | bit : S.inflight & ~bit;
-                S.inflight_par = ((it + 1) >> 1) & 1 ? S.inflight_par | bit : S.inflight_par & ~bit;
+                S.inflight = produce(a, total, S) ? 1u : 0u;
+                S.inflight_par = it & 1;
             } else {
                 atomicOr(&a.counters[2], 1ull);
                 S.fail = 1;
             }
         }
         // every exit is taken by whole warps (record flushes use the full warp)
-        const bool got = mbar_wait(&S.full[b], (it >> 1) & 1);
-        if (tid == 0 && got) S.inflight &= ~(1u << b);
+        const bool got = mbar_wait(&S.full, it & 1);
+        if (tid == 0 && got) S.inflight = 0;
         if (!__all_sync(kFull, got)) {
             if (lane == 0) atomicOr(&a.counters[2], 2ull);
             break;
         }
-        const uint32_t item = S.item[b];
+        const uint32_t item = S.item;
         if (__any_sync(kFull, item >= total || S.fail)) break;
         const ItemRef r = locate(a, item);
         if (COUNT) ++w_items;
@@ -390,36 +404,40 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
             item_c0 = clock64();
             item_recs0 = w_recs;
         }
-        const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[b].q);
-        const uint32_t *sz = S.st[b].z;
         for (uint32_t t0 = r.tb + warp * kQuad; t0 < r.te; t0 += kMatchWarps * kQuad) {
-            // selection for four tiles at once: lane l serves word l & 7 of
-            // tile t0 + (l >> 3); the tile's 8 selector bits OR the "lacks"
-            // slices of the lane's 32 queries
-            const uint32_t gi = lane >> 3, w = lane & 7;
+            // selection for two tiles and both chunks at once: lane l serves
+            // word l & 7 of chunk (l >> 3) & 1 for tile t0 + (l >> 4); the
+            // tile's 8 selector bits OR the "lacks" slices of the lane's 32
+            // queries
+            const uint32_t gi = lane >> 4, ch = (lane >> 3) & 1, w = lane & 7, tl = lane & 15;
             const uint32_t tq = t0 + gi;
+            uint32_t nqc = r.nq[0];  // queries in the lane's chunk (no dynamic index into r)
+#pragma unroll
+            for (int c = 1; c < kItemChunks; ++c)
+                if (ch == (uint32_t)c) nqc = r.nq[c];
             uint32_t cand = 0, tcount = 0;
             if (tq < r.te) {
                 const TileInfo ti = a.tile_info[tq];
                 tcount = ti.count;
-                const uint32_t *zl = sz + w;
+                const uint32_t *zl = S.st[ch].z + w;
                 const uint32_t lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
                                       zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] |
                                       zl[(ti.sel[1] & 0xFFu) * 8] | zl[((ti.sel[1] >> 8) & 0xFFu) * 8] |
                                       zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
                 cand = ~lack;
-                if (w * 32 + 32 > r.nq) cand &= w * 32 >= r.nq ? 0u : ((1u << (r.nq - w * 32)) - 1u);
-                if (w == 0) S.tk[warp][gi] = a.tile_keys[tq];
+                if (w * 32 + 32 > nqc) cand &= w * 32 >= nqc ? 0u : ((1u << (nqc - w * 32)) - 1u);
+                if (tl == 0) S.tk[warp][gi] = a.tile_keys[tq];
             }
-            if (COUNT) w_tiles += __popc(__ballot_sync(kFull, tq < r.te && w == 0));  // lane 0 reports
-            // candidate lists (query index in the chunk, one byte each): a
-            // prefix sum over each tile's 8 words places every lane's queries
+            if (COUNT) w_tiles += __popc(__ballot_sync(kFull, tq < r.te && tl == 0));  // lane 0 reports
+            // candidate lists (query index in its chunk, one byte each): a
+            // prefix sum over each tile's 16 words (the first chunk's 8,
+            // then the second's) places every lane's queries
             const uint32_t cnt = __popc(cand);
             uint32_t incl = cnt;
 #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
+            for (int o = 1; o < 16; o <<= 1) {
                 const uint32_t v = __shfl_up_sync(kFull, incl, o);
-                if (w >= (unsigned)o) incl += v;
+                if (tl >= (unsigned)o) incl += v;
             }
             {
                 uint8_t *lst = S.list[warp][gi];
@@ -428,16 +446,17 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                     lst[pos++] = uint8_t(w * 32 + __ffs(cand) - 1);
                     cand &= cand - 1;
                 }
-                const uint32_t nt = __shfl_sync(kFull, incl, lane | 7);
-                if (w < 4) lst[nt + w] = 0;  // pad to a multiple of 4 (query 0; its hits are dropped)
+                const uint32_t nt = __shfl_sync(kFull, incl, lane | 15);
+                if (tl < 4) lst[nt + tl] = 0;  // pad to a multiple of 4 (its hits are dropped)
             }
             __syncwarp();
             for (int i = 0; i < kQuad; ++i) {
-                const uint32_t n = __shfl_sync(kFull, incl, 8 * i + 7);
+                const uint32_t n = __shfl_sync(kFull, incl, 16 * i + 15);
+                const uint32_t n0 = __shfl_sync(kFull, incl, 16 * i + 7);  // list entries of the first chunk
                 if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
                 if (n == 0) continue;
                 const uint32_t t = t0 + i;
-                const uint32_t count = __shfl_sync(kFull, tcount, 8 * i);
+                const uint32_t count = __shfl_sync(kFull, tcount, 16 * i);
                 const uint8_t *lst = S.list[warp][i];
                 uint32_t f[kWords];
 #pragma unroll
@@ -457,6 +476,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                             if (p0 == 0 && n <= 16) ++w_small;
                         }
                         const uint32_t j = p0 + lane;
+                        const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[j < n0 ? 0 : 1].q);
                         const uint32_t c2 = j < n ? 2u * lst[j] : 0u;
                         const uint4 qa = sq[c2], qb = sq[c2 + 1];
                         uint32_t m = 0;
@@ -515,10 +535,15 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                         const uint32_t idx4 = *reinterpret_cast<const uint32_t *>(lst + j);
                         const uint32_t ia = (idx4 & 0xFFu) * 2, ib = ((idx4 >> 8) & 0xFFu) * 2;
                         const uint32_t ic = ((idx4 >> 16) & 0xFFu) * 2, id = (idx4 >> 24) * 2;
-                        const uint4 p0 = sq[ia], p1 = sq[ia + 1];
-                        const uint4 q0 = sq[ib], q1 = sq[ib + 1];
-                        const uint4 r0 = sq[ic], r1 = sq[ic + 1];
-                        const uint4 u0 = sq[id], u1 = sq[id + 1];
+                        // candidate j + k is in the first chunk's buffer when j + k < n0
+                        const uint4 *sa = reinterpret_cast<const uint4 *>(S.st[j < n0 ? 0 : 1].q);
+                        const uint4 *sb = reinterpret_cast<const uint4 *>(S.st[j + 1 < n0 ? 0 : 1].q);
+                        const uint4 *sc = reinterpret_cast<const uint4 *>(S.st[j + 2 < n0 ? 0 : 1].q);
+                        const uint4 *sd = reinterpret_cast<const uint4 *>(S.st[j + 3 < n0 ? 0 : 1].q);
+                        const uint4 p0 = sa[ia], p1 = sa[ia + 1];
+                        const uint4 q0 = sb[ib], q1 = sb[ib + 1];
+                        const uint4 r0 = sc[ic], r1 = sc[ic + 1];
+                        const uint4 u0 = sd[id], u1 = sd[id + 1];
                         uint32_t x0 = f[0] & ~p0.x, x1 = f[0] & ~q0.x, x2 = f[0] & ~r0.x, x3 = f[0] & ~u0.x;
                         x0 = andnot_or(f[1], p0.y, x0);
                         x1 = andnot_or(f[1], q0.y, x1);
@@ -577,7 +602,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
             atomicAdd(&a.item_stats[2 * size_t(item)], (unsigned long long)(clock64() - item_c0));
             atomicAdd(&a.item_stats[2 * size_t(item) + 1], (unsigned long long)(w_recs - item_recs0));
         }
-        if (lane == 0) mbar_arrive(&S.empty[b]);
+        if (lane == 0) mbar_arrive(&S.empty);
     }
     if (wn) flush_recs(S.rec[warp], wn, a, lane);
     pairs = __reduce_add_sync(kFull, pairs);
@@ -594,11 +619,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     }
     // no copy may still target this CTA's shared memory when it exits: after
     // a failed wait, wait (bounded) for the copies still in flight
-    if (tid == 0) {
-        for (int s = 0; s < 2; ++s)
-            if (((S.inflight >> s) & 1) && !mbar_wait(&S.full[s], (S.inflight_par >> s) & 1))
-                atomicOr(&a.counters[2], 4ull);
-    }
+    if (tid == 0 && S.inflight && !mbar_wait(&S.full, S.inflight_par)) atomicOr(&a.counters[2], 4ull);
 }
 
 // Launches the subset test on grid CTAs (its shared memory is above the

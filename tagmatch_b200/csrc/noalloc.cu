@@ -80,7 +80,8 @@ struct Arena {
     }
 };
 
-// Work-plan counts per partition: 256-query chunks, and chunks x tile segments.
+// Work-plan counts per partition: 256-query chunks, and work items (groups
+// of kItemChunks chunks x tile segments).
 __global__ void k_plan_counts(const uint32_t *__restrict__ part_count, const uint32_t *__restrict__ part_tile_begin,
                               uint32_t n_parts, uint32_t seg_tiles, uint32_t *__restrict__ nchunks,
                               uint32_t *__restrict__ nitems) {
@@ -89,7 +90,7 @@ __global__ void k_plan_counts(const uint32_t *__restrict__ part_count, const uin
     const uint32_t c = (part_count[p] + kChunk - 1) / kChunk;
     const uint32_t nt = part_tile_begin[p + 1] - part_tile_begin[p];
     nchunks[p] = c;
-    nitems[p] = c * ((nt + seg_tiles - 1) / seg_tiles);
+    nitems[p] = ((c + kItemChunks - 1) / kItemChunks) * ((nt + seg_tiles - 1) / seg_tiles);
 }
 
 // Exclusive scan with block sums held in the arena (up to 2048 x 2048 elements).

@@ -392,7 +392,7 @@ void item_features(float *x, uint32_t part_size, uint32_t mask_bits, uint32_t qu
     x[0] = std::log2(1.f + float(part_size)) / 16.f;
     x[1] = float(mask_bits) / 32.f;
     x[2] = std::log2(1.f + float(queued)) / 18.f;
-    x[3] = float(chunk_queries) / float(kChunk);
+    x[3] = float(chunk_queries) / float(kItemQueries);
     x[4] = std::log2(1.f + float(seg_tiles_here)) / 13.f;
     x[5] = density * 100.f;
     x[6] = float(part_size) / (float(kTile) * float(std::max<uint32_t>(part_tiles, 1)));
@@ -464,12 +464,12 @@ void Scheduler::absorb(const DevTable &t, const MatchScratch &s, uint32_t nq, do
             batch_density[p] = cnt && tiles ? float(double(recs) / (double(cnt) * tiles)) : 0.f;
             if (i1 == i0) continue;
             const float dens = density_[p] >= 0.f ? density_[p] : batch_density[p];
-            const uint32_t nch = (cnt + kChunk - 1) / kChunk;
+            const uint32_t nch = (cnt + kItemQueries - 1) / kItemQueries;  // chunk groups
             for (uint32_t i = i0; i < i1 && t_.size() < kMaxSamples; ++i) {
                 const unsigned long long cyc = s.h_item_stats[2 * size_t(i)];
                 if (cyc == 0) continue;
                 const uint32_t local = i - i0, chunk = local % nch, sg = local / nch;
-                const uint32_t cq = std::min<uint32_t>(kChunk, cnt - chunk * kChunk);
+                const uint32_t cq = std::min<uint32_t>(kItemQueries, cnt - chunk * kItemQueries);
                 const uint32_t ts = std::min<uint32_t>(seg, tiles - sg * seg);
                 float f[kMlpIn];
                 item_features(f, t.h_part_size[p], mask_bits(t, p), cnt, cq, ts, dens, tiles, seg);
@@ -506,7 +506,7 @@ TrainReport Scheduler::train(const DevTable &t, uint32_t seg_tiles, int sm_count
 void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, double clock_hz, cudaStream_t st) {
     const uint32_t P = t.n_parts;
     if (P == 0 || frac_.size() != P || !model_.trained()) return;
-    // rows: [s][k][p][full chunk, partial chunk], then the order rows [p]
+    // rows: [s][k][p][full item, partial item], then the order rows [p]
     const size_t per_seg = size_t(kTableSteps) * P * 2;
     const size_t rows = size_t(kSegChoices) * per_seg + P;
     std::vector<float> x(rows * kMlpIn), y(rows);
@@ -521,9 +521,10 @@ void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, do
                 const uint32_t cnt = uint32_t(std::llround(b * frac_[p]));
                 const float dens = std::max(density_[p], 0.f);
                 const size_t r0 = size_t(si) * per_seg + (size_t(k) * P + p) * 2;
-                item_features(&x[r0 * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt, kChunk, ts, dens, tiles, sg);
+                item_features(&x[r0 * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt, kItemQueries, ts, dens, tiles,
+                              sg);
                 item_features(&x[(r0 + 1) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt,
-                              std::max<uint32_t>(1, cnt % kChunk), ts, dens, tiles, sg);
+                              std::max<uint32_t>(1, cnt % kItemQueries), ts, dens, tiles, sg);
             }
         }
     }
@@ -535,7 +536,7 @@ void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, do
         const uint32_t ns = std::max<uint32_t>(1, (tiles + seg - 1) / seg);
         const uint32_t cnt = uint32_t(std::llround(ref_b * frac_[p]));
         item_features(&x[(size_t(kSegChoices) * per_seg + p) * kMlpIn], t.h_part_size[p], mask_bits(t, p), cnt,
-                      std::min<uint32_t>(kChunk, std::max<uint32_t>(cnt, 1)), (tiles + ns - 1) / ns,
+                      std::min<uint32_t>(kItemQueries, std::max<uint32_t>(cnt, 1)), (tiles + ns - 1) / ns,
                       std::max(density_[p], 0.f), tiles, seg);
     }
     model_.predict(x.data(), rows, y.data(), st);
@@ -551,7 +552,7 @@ void Scheduler::refresh_locked(const DevTable &t, uint32_t seg, int sm_count, do
                 const uint32_t ns = std::max<uint32_t>(1, (tiles + sg - 1) / sg);
                 const size_t r0 = size_t(si) * per_seg + (size_t(k) * P + p) * 2;
                 const uint32_t cnt = uint32_t(std::llround(double(cnt_scale) * frac_[p]));
-                const uint32_t nf = cnt / kChunk, rm = cnt % kChunk;
+                const uint32_t nf = cnt / kItemQueries, rm = cnt % kItemQueries;
                 const double cf = std::exp(double(y[r0])), cr = rm ? std::exp(double(y[r0 + 1])) : 0.0;
                 cyc += double(ns) * (nf * cf + cr);
                 if (nf) longest = std::max(longest, cf);
