@@ -13,7 +13,9 @@ constexpr int kRouteThreads = 256;
 constexpr int kMatchThreads = 256;
 constexpr int kMatchWarps = kMatchThreads / 32;
 constexpr int kWarpRecs = 64;  // staged hit records per warp (1 KB)
-constexpr int kQuad = 2;       // tiles a warp selects candidates for at once (for both chunks of its item)
+constexpr int kQuad = 1;       // tiles a warp selects candidates for at once (for all chunks of its item)
+constexpr int kTileLanes = 32 / kQuad;  // lanes per tile in the selection: 8 words x kItemChunks chunks
+static_assert(kTileLanes == 8 * kItemChunks, "selection lanes");
 constexpr uint32_t kMaxRouteParts = 1536;  // partition masks per routing window (48 KB of shared memory)
 constexpr unsigned long long kSpinLimit = 1ull << 26;
 
@@ -218,21 +220,17 @@ struct MatchArgs {
 
 constexpr int kSliceWords = kSliceRows * 8;  // 193 x 256 bits
 
-// One staging buffer: a chunk's query records and slices.
-// The query array has one record past the chunk: the pad record (all
-// words zero, query id kPadQuery) that candidate-list padding points at.
+// A chunk's staged query records (8 KB), and one record past the chunk:
+// the pad record (all words zero, query id kPadQuery).
 constexpr uint32_t kPadQuery = 0xFFFFFFFFu;
-struct __align__(128) Stage {
-    uint32_t q[(kChunk + 1) * kQueueWords];  // 8 KB + the pad record
-    uint32_t z[kSliceWords];                 // 6 KB
-};
+constexpr int kStageWords = (kChunk + 1) * kQueueWords;
 
 // Shared memory of one matcher CTA (dynamic; ~51 KB, 4 CTAs per SM).
 struct MatchSmem {
-    Stage st[kItemChunks];                               // the item's chunks
+    uint32_t q[kItemChunks][kStageWords];                // the item's chunks' query records
     HitRec rec[kMatchWarps][kWarpRecs];                  // staged hit records per warp
-    // candidate lists per warp and tile: the first chunk's candidates, then
-    // the second's (query index in its chunk), padded to a multiple of 4
+    // candidate lists per warp and tile: the chunks' candidates in chunk
+    // order (query index in its chunk), padded to a multiple of 4
     uint8_t list[kMatchWarps][kQuad][kItemQueries + 8];
     TileKeys tk[kMatchWarps][kQuad];                     // key-count planes of the warp's tiles
     uint4 tf[kMatchWarps][kWords][kTile / 4];            // a warp's tile: word k of filters 4 g .. 4 g + 3
@@ -243,6 +241,9 @@ struct MatchSmem {
     // that completes it
     uint32_t inflight, inflight_par;
 };
+
+// 4 CTAs per SM: 228 KB of shared memory per SM, 1 KB of it reserved per CTA
+static_assert(4 * (sizeof(MatchSmem) + 1024) <= 228 * 1024, "the matcher's shared memory must fit 4 CTAs per SM");
 
 // Moves a warp's n staged records to the global record buffer (one atomic
 // reserves their place; past the capacity they are only counted, and the
@@ -292,8 +293,8 @@ __device__ __forceinline__ ItemRef locate(const MatchArgs &a, uint32_t item) {
 }
 
 // Thread 0: claim the next item and start the copies of its chunks' query
-// records and slices; the item id is published through the full barrier's
-// phase completion.  Returns whether copies are in flight.
+// records; the item id is published through the full barrier's phase
+// completion.  Returns whether copies are in flight.
 __device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, MatchSmem &S) {
     const uint32_t item = uint32_t(atomicAdd(&a.counters[0], 1ull));
     S.item = item;
@@ -301,17 +302,14 @@ __device__ __forceinline__ bool produce(const MatchArgs &a, uint32_t total, Matc
         const ItemRef r = locate(a, item);
         uint32_t bytes = 0;
 #pragma unroll
-        for (int c = 0; c < kItemChunks; ++c)
-            if (r.nq[c]) bytes += r.nq[c] * kQueueWords * sizeof(uint32_t) + kSliceWords * sizeof(uint32_t);
+        for (int c = 0; c < kItemChunks; ++c) bytes += r.nq[c] * kQueueWords * sizeof(uint32_t);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         mbar_expect_tx(&S.full, bytes);
 #pragma unroll
         for (int c = 0; c < kItemChunks; ++c) {
             if (!r.nq[c]) continue;
-            tma_bulk_g2s(S.st[c].q, a.queue + (size_t(r.qbase) + size_t(c) * kChunk) * kQueueWords,
+            tma_bulk_g2s(S.q[c], a.queue + (size_t(r.qbase) + size_t(c) * kChunk) * kQueueWords,
                          r.nq[c] * kQueueWords * sizeof(uint32_t), &S.full);
-            tma_bulk_g2s(S.st[c].z, a.slices + (size_t(r.zchunk) + c) * kSliceWords, kSliceWords * sizeof(uint32_t),
-                         &S.full);
         }
         return true;
     }
@@ -354,7 +352,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     const uint32_t total = a.item_off[a.n_parts];
     if (tid < kItemChunks * kQueueWords) {
         const uint32_t k = tid % kQueueWords;
-        S.st[tid / kQueueWords].q[kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
+        S.q[tid / kQueueWords][kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
     }
     if (tid == 0) {
         mbar_init(&S.full, 1);
@@ -405,11 +403,12 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
             item_recs0 = w_recs;
         }
         for (uint32_t t0 = r.tb + warp * kQuad; t0 < r.te; t0 += kMatchWarps * kQuad) {
-            // selection for two tiles and both chunks at once: lane l serves
-            // word l & 7 of chunk (l >> 3) & 1 for tile t0 + (l >> 4); the
-            // tile's 8 selector bits OR the "lacks" slices of the lane's 32
-            // queries
-            const uint32_t gi = lane >> 4, ch = (lane >> 3) & 1, w = lane & 7, tl = lane & 15;
+            // selection for the warp's tiles and all chunks of the item at
+            // once: lane l serves word l & 7 of chunk (l >> 3) % kItemChunks
+            // for tile t0 + l / kTileLanes; the tile's 8 selector bits OR the
+            // "lacks" slices of the lane's 32 queries (read through L1: the
+            // item's slices are shared by all its tiles)
+            const uint32_t gi = lane / kTileLanes, tl = lane % kTileLanes, ch = tl >> 3, w = lane & 7;
             const uint32_t tq = t0 + gi;
             uint32_t nqc = r.nq[0];  // queries in the lane's chunk (no dynamic index into r)
 #pragma unroll
@@ -419,23 +418,26 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
             if (tq < r.te) {
                 const TileInfo ti = a.tile_info[tq];
                 tcount = ti.count;
-                const uint32_t *zl = S.st[ch].z + w;
-                const uint32_t lack = zl[(ti.sel[0] & 0xFFu) * 8] | zl[((ti.sel[0] >> 8) & 0xFFu) * 8] |
-                                      zl[((ti.sel[0] >> 16) & 0xFFu) * 8] | zl[(ti.sel[0] >> 24) * 8] |
-                                      zl[(ti.sel[1] & 0xFFu) * 8] | zl[((ti.sel[1] >> 8) & 0xFFu) * 8] |
-                                      zl[((ti.sel[1] >> 16) & 0xFFu) * 8] | zl[(ti.sel[1] >> 24) * 8];
-                cand = ~lack;
-                if (w * 32 + 32 > nqc) cand &= w * 32 >= nqc ? 0u : ((1u << (nqc - w * 32)) - 1u);
+                if (nqc) {  // chunks past the partition's last have no slices
+                    const uint32_t *zl = a.slices + (size_t(r.zchunk) + ch) * kSliceWords + w;
+                    const uint32_t lack =
+                        __ldg(&zl[(ti.sel[0] & 0xFFu) * 8]) | __ldg(&zl[((ti.sel[0] >> 8) & 0xFFu) * 8]) |
+                        __ldg(&zl[((ti.sel[0] >> 16) & 0xFFu) * 8]) | __ldg(&zl[(ti.sel[0] >> 24) * 8]) |
+                        __ldg(&zl[(ti.sel[1] & 0xFFu) * 8]) | __ldg(&zl[((ti.sel[1] >> 8) & 0xFFu) * 8]) |
+                        __ldg(&zl[((ti.sel[1] >> 16) & 0xFFu) * 8]) | __ldg(&zl[(ti.sel[1] >> 24) * 8]);
+                    cand = ~lack;
+                    if (w * 32 + 32 > nqc) cand &= w * 32 >= nqc ? 0u : ((1u << (nqc - w * 32)) - 1u);
+                }
                 if (tl == 0) S.tk[warp][gi] = a.tile_keys[tq];
             }
             if (COUNT) w_tiles += __popc(__ballot_sync(kFull, tq < r.te && tl == 0));  // lane 0 reports
             // candidate lists (query index in its chunk, one byte each): a
-            // prefix sum over each tile's 16 words (the first chunk's 8,
-            // then the second's) places every lane's queries
+            // prefix sum over each tile's words (chunk by chunk) places every
+            // lane's queries
             const uint32_t cnt = __popc(cand);
             uint32_t incl = cnt;
 #pragma unroll
-            for (int o = 1; o < 16; o <<= 1) {
+            for (int o = 1; o < kTileLanes; o <<= 1) {
                 const uint32_t v = __shfl_up_sync(kFull, incl, o);
                 if (tl >= (unsigned)o) incl += v;
             }
@@ -446,17 +448,27 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                     lst[pos++] = uint8_t(w * 32 + __ffs(cand) - 1);
                     cand &= cand - 1;
                 }
-                const uint32_t nt = __shfl_sync(kFull, incl, lane | 15);
+                const uint32_t nt = __shfl_sync(kFull, incl, lane | (kTileLanes - 1));
                 if (tl < 4) lst[nt + tl] = 0;  // pad to a multiple of 4 (its hits are dropped)
             }
             __syncwarp();
             for (int i = 0; i < kQuad; ++i) {
-                const uint32_t n = __shfl_sync(kFull, incl, 16 * i + 15);
-                const uint32_t n0 = __shfl_sync(kFull, incl, 16 * i + 7);  // list entries of the first chunk
+                const uint32_t n = __shfl_sync(kFull, incl, kTileLanes * i + kTileLanes - 1);
+                // list positions where chunks 1 .. kItemChunks - 1 begin: the
+                // candidate at position x is in chunk sum_c (x >= cb[c])
+                uint32_t cb[kItemChunks - 1];
+#pragma unroll
+                for (int c = 0; c + 1 < kItemChunks; ++c) cb[c] = __shfl_sync(kFull, incl, kTileLanes * i + 8 * c + 7);
+                auto chunk_of = [&](uint32_t x) {
+                    uint32_t c = 0;
+#pragma unroll
+                    for (int k = 0; k + 1 < kItemChunks; ++k) c += x >= cb[k] ? 1u : 0u;
+                    return c;
+                };
                 if (COUNT) w_cand += n;  // the warp's candidates (lane 0 reports)
                 if (n == 0) continue;
                 const uint32_t t = t0 + i;
-                const uint32_t count = __shfl_sync(kFull, tcount, 16 * i);
+                const uint32_t count = __shfl_sync(kFull, tcount, kTileLanes * i);
                 const uint8_t *lst = S.list[warp][i];
                 uint32_t f[kWords];
 #pragma unroll
@@ -476,7 +488,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                             if (p0 == 0 && n <= 16) ++w_small;
                         }
                         const uint32_t j = p0 + lane;
-                        const uint4 *sq = reinterpret_cast<const uint4 *>(S.st[j < n0 ? 0 : 1].q);
+                        const uint4 *sq = reinterpret_cast<const uint4 *>(S.q[chunk_of(j)]);
                         const uint32_t c2 = j < n ? 2u * lst[j] : 0u;
                         const uint4 qa = sq[c2], qb = sq[c2 + 1];
                         uint32_t m = 0;
@@ -535,11 +547,10 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                         const uint32_t idx4 = *reinterpret_cast<const uint32_t *>(lst + j);
                         const uint32_t ia = (idx4 & 0xFFu) * 2, ib = ((idx4 >> 8) & 0xFFu) * 2;
                         const uint32_t ic = ((idx4 >> 16) & 0xFFu) * 2, id = (idx4 >> 24) * 2;
-                        // candidate j + k is in the first chunk's buffer when j + k < n0
-                        const uint4 *sa = reinterpret_cast<const uint4 *>(S.st[j < n0 ? 0 : 1].q);
-                        const uint4 *sb = reinterpret_cast<const uint4 *>(S.st[j + 1 < n0 ? 0 : 1].q);
-                        const uint4 *sc = reinterpret_cast<const uint4 *>(S.st[j + 2 < n0 ? 0 : 1].q);
-                        const uint4 *sd = reinterpret_cast<const uint4 *>(S.st[j + 3 < n0 ? 0 : 1].q);
+                        const uint4 *sa = reinterpret_cast<const uint4 *>(S.q[chunk_of(j)]);
+                        const uint4 *sb = reinterpret_cast<const uint4 *>(S.q[chunk_of(j + 1)]);
+                        const uint4 *sc = reinterpret_cast<const uint4 *>(S.q[chunk_of(j + 2)]);
+                        const uint4 *sd = reinterpret_cast<const uint4 *>(S.q[chunk_of(j + 3)]);
                         const uint4 p0 = sa[ia], p1 = sa[ia + 1];
                         const uint4 q0 = sb[ib], q1 = sb[ib + 1];
                         const uint4 r0 = sc[ic], r1 = sc[ic + 1];

@@ -14,7 +14,7 @@ constexpr int kWords = 6;          // 32-bit words per filter
 constexpr int kBits = 192;         // filter width
 constexpr int kTile = 32;          // filters per tile (one per lane of a warp)
 constexpr int kChunk = 256;        // queries per partition batch (QUERIES_BATCH_SIZE, parameters.hh:13)
-constexpr int kItemChunks = 2;     // 256-query chunks of one partition that a subset-test work item covers
+constexpr int kItemChunks = 4;     // 256-query chunks of one partition that a subset-test work item covers
 constexpr int kItemQueries = kItemChunks * kChunk;
 constexpr int kQueueWords = 8;     // queued query record: 6 filter words, query id, pad (32 bytes)
 constexpr unsigned kFull = 0xFFFFFFFFu;
