@@ -15,23 +15,21 @@
 //                shared memory); CTA-local counts reserve queue space with
 //                one global atomic per (CTA, partition); queue records are
 //                32 bytes (6 query words, query id, pad);
-//   host plan    work items = (partition, 256-query chunk, segment of the
-//                partition's tiles), offsets computed on the host from the
-//                per-partition counts, partitions in id order or in the
-//                order the learned cost model gives;
+//   host plan    work items = (partition, group of four 256-query chunks,
+//                segment of the partition's tiles), offsets computed on the
+//                host from the per-partition counts, partitions in id order
+//                or in the order the learned cost model gives;
 //   k_slices     per 256-query chunk, bit-sliced "lacks bit b" masks:
 //                Z[b] bit j set when query j of the chunk lacks bit b
 //                (192 x 256 bits, ballot per bit);
 //   k_match      persistent CTAs take items from an atomic counter.  Each
-//                item's queries and slices are staged into shared memory by
-//                bulk TMA copies (cp.async.bulk + mbarrier), double-buffered:
-//                the next item loads while this one is matched, and the
-//                buffer is released by per-warp mbarrier arrivals instead of
-//                a CTA barrier.  Each warp takes four tiles of <= 32 filters;
-//                each tile's AND mask selects candidate queries by OR-ing the
-//                slices of its bits (8 lanes per tile, one 32-query word
-//                each); the
-//                candidates are tested either one per lane against the
+//                item's query records are staged into shared memory by bulk
+//                TMA copies (cp.async.bulk + mbarrier), one per chunk; the
+//                buffers are released by per-warp mbarrier arrivals.  A warp
+//                takes one tile of <= 32 filters at a time; the tile's AND
+//                mask selects candidate queries of all four chunks by
+//                OR-ing the slices of its bits (one 32-query word per lane);
+//                the candidates are tested either one per lane against the
 //                tile's filters broadcast from shared memory, or, when they
 //                are few, four at a time against the tile held one filter
 //                per lane (6 LOP3s per (query, filter) either way); each
@@ -40,8 +38,9 @@
 //                flushed with one global atomic, and its key count is added
 //                to the query's total;
 //   k_key_fill   after a prefix sum of the query totals: one cursor atomic
-//                per record, then one contiguous key range per run of hit
-//                bits, four records per lane in flight;
+//                per record; the runs of adjacent hit bits of a warp's 64
+//                records (one key range each) are numbered and copied 32 at
+//                a time by the whole warp;
 //   k_unique_*   match_unique: per-query bitmap (small key spaces, output
 //                comes out sorted) or per-query block radix sort + unique.
 // Result overflow is exact: the record buffer is regrown and the batch re-run

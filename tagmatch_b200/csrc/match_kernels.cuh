@@ -606,7 +606,7 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
                 }
                 __syncwarp();  // the tile buffer is rebuilt for the next tile
             }
-            __syncwarp();  // the lists are rebuilt for the next four tiles
+            __syncwarp();  // the lists are rebuilt for the next tiles
         }
         __syncwarp();
         if (TIMED && lane == 0) {
