@@ -257,9 +257,9 @@ int tm_mlp_loss_grad(const float *params, const float *features, const float *ta
                      float *grad, float *loss);
 
 /* Tiles per work item of the subset test (what tm_autotune chooses;
- * default 128): each work item is one 256-query chunk of a partition
- * against this many of its tiles (up to 32 filters each).  No reference
- * counterpart.  Results do not depend on it. */
+ * default 128): each work item is a group of four consecutive 256-query
+ * chunks of a partition against this many of its tiles (up to 32 filters
+ * each).  No reference counterpart.  Results do not depend on it. */
 int tm_set_tiles_per_item(tm_engine *e, uint32_t seg_tiles);
 uint32_t tm_get_tiles_per_item(const tm_engine *e);
 
