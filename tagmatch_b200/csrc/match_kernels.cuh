@@ -220,12 +220,12 @@ struct MatchArgs {
 
 constexpr int kSliceWords = kSliceRows * 8;  // 193 x 256 bits
 
-// A chunk's staged query records (8 KB), and one record past the chunk:
-// the pad record (all words zero, query id kPadQuery).
+// A chunk's staged query records (8 KB).  kPadQuery marks the gather's
+// padding records (no query).
 constexpr uint32_t kPadQuery = 0xFFFFFFFFu;
-constexpr int kStageWords = (kChunk + 1) * kQueueWords;
+constexpr int kStageWords = kChunk * kQueueWords;
 
-// Shared memory of one matcher CTA (dynamic; ~51 KB, 4 CTAs per SM).
+// Shared memory of one matcher CTA (dynamic; ~54 KB, 4 CTAs per SM).
 struct MatchSmem {
     uint32_t q[kItemChunks][kStageWords];                // the item's chunks' query records
     HitRec rec[kMatchWarps][kWarpRecs];                  // staged hit records per warp
@@ -350,10 +350,6 @@ __global__ void __launch_bounds__(kMatchThreads, 4) k_match(MatchArgs a) {  // 4
     MatchSmem &S = *reinterpret_cast<MatchSmem *>(smem_raw);
     const unsigned tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t total = a.item_off[a.n_parts];
-    if (tid < kItemChunks * kQueueWords) {
-        const uint32_t k = tid % kQueueWords;
-        S.q[tid / kQueueWords][kChunk * kQueueWords + k] = k == 6 ? kPadQuery : 0u;
-    }
     if (tid == 0) {
         mbar_init(&S.full, 1);
         mbar_init(&S.empty, kMatchWarps);
