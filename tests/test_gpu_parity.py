@@ -182,6 +182,20 @@ def test_many_queries_one_partition_chunks():
     tm.close()
 
 
+@pytest.mark.parametrize("nq", [1, 255, 256, 257, 767, 1023, 1024, 1025, 2049, 3333])
+def test_work_item_chunk_groups(nq):
+    """A work item covers up to four 256-query chunks of a partition: query
+    counts on both sides of the chunk and item boundaries, the last item
+    holding 1 to 4 chunks, each chunk full or partial."""
+    f, ko, k = workload.generate_filters(3000, 43)
+    q = workload.generate_queries(nq, f, 43 + nq, superset_fraction=0.9)
+    tm = engine_with(f, ko, k, 65536)
+    off, keys = tm.match_batch(q)
+    ooff, okeys = oracle.match(f, ko, k, q)
+    assert_same_multisets(off, keys, ooff, okeys)
+    tm.close()
+
+
 def test_capacity_error_reports_required_size():
     f, ko, k = workload.generate_filters(2000, 42)
     q = workload.generate_queries(100, f, 42)
